@@ -1,0 +1,244 @@
+/*
+ * tpm.h -- C ABI of tigerpm_b200, a B200-native (sm_100a) PME kick.
+ *
+ * The library replaces the reference's PME kick path: the chain-mesh cell
+ * sort, the long-range PM solve and the fused interpolation / short-range PP /
+ * rung-kick kernel, plus the FP64 Ewald comparison.  Every entry point names
+ * the reference interface it stands in for (paths relative to the
+ * dmarce1/tigerpm tree).  The reference has no C ABI: its interfaces are C++
+ * free functions over global state, kept as C++ wrappers in
+ * include/tpm_reference.hpp on top of these calls.
+ *
+ * Conventions
+ *  - Every call returns int: TPM_OK (0) or a negative TPM_ERR_* code.  Nothing
+ *    aborts or traps; tpm_error_string() and tpm_last_error_message() explain.
+ *  - A tpm_ctx holds ONE periodic box: its particles, chain mesh, PM grid,
+ *    cuFFT plans and scratch live in device memory owned by the context and
+ *    persist across calls.  Host pointers passed in are owned by the caller
+ *    and only read/written during the call.
+ *  - Positions are the reference's fixed32: raw uint32 = floor(x * 2^32),
+ *    uint32 wrap-around being the periodic boundary (tigerpm/fixed.hpp).
+ *  - Particle arrays are in the context's current order; tpm_chainmesh_create
+ *    permutes them into chain-mesh order, exactly as the reference's
+ *    chainmesh_create permutes particles_X/U/R.
+ *  - One host thread per context at a time.  All work is issued on the
+ *    context's CUDA stream; calls that return host data synchronise it.
+ */
+#ifndef TPM_H_
+#define TPM_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define TPM_OK 0
+#define TPM_ERR_INVALID (-1)       /* bad argument or option combination */
+#define TPM_ERR_NOMEM (-2)         /* device or host allocation failed */
+#define TPM_ERR_CUDA (-3)          /* a CUDA runtime call failed */
+#define TPM_ERR_CUFFT (-4)         /* a cuFFT call failed */
+#define TPM_ERR_STATE (-5)         /* call out of order (e.g. kick before sort) */
+#define TPM_ERR_RUNG (-6)          /* a new rung fell outside [0, 32) (clamped) */
+#define TPM_ERR_CAPACITY (-7)      /* particle count above the context capacity */
+#define TPM_ERR_BUDGET (-8)        /* request exceeds the admitted HBM budget */
+#define TPM_ERR_TIMEOUT (-9)       /* a bounded device wait gave up */
+#define TPM_ERR_NOEXT (-10)        /* library built without a required part */
+
+/* gravity_long_type (tigerpm/gravity_long.hpp:13-15) */
+#define TPM_GRAVITY_LONG_PM 0
+#define TPM_GRAVITY_LONG_PME 1
+
+/* mass assignment: cloud4 = the reference's cubic B-spline deposit
+ * (src/gravity_long.cpp:127-199); CIC and TSC are extensions. */
+#define TPM_ASSIGN_CLOUD4 0
+#define TPM_ASSIGN_CIC 1
+#define TPM_ASSIGN_TSC 2
+
+/* chain-mesh order: PARITY replays the reference's recursive partition and
+ * reproduces its within-cell order bit for bit (src/chainmesh.cpp:168-213,
+ * src/particles.cpp:414-444); FAST is a stable counting sort with the same
+ * cell offsets and input order inside each cell. */
+#define TPM_SORT_PARITY 0
+#define TPM_SORT_FAST 1
+
+/*
+ * Options.  The first block mirrors struct options (tigerpm/options.hpp:6-27)
+ * field for field; tpm_options_init derives it as process_options does
+ * (src/options.cpp:81-96).  The second block holds this library's extensions;
+ * zero / negative values select the reference behaviour.
+ */
+typedef struct tpm_options {
+  int four_dim;     /* PM grid points per side */
+  int chain_dim;    /* chain-mesh cells per side */
+  int parts_dim;    /* particles^(1/3) */
+  int parts_o_four;
+  int parts_o_chain;
+  int four_o_chain;
+  double eta;
+  double sigma8;
+  double code_to_cm;
+  double hubble;
+  double GM;
+  double hsoft;     /* softening length, box units */
+  double box_size;
+  double rs;        /* PME split scale, box units (reference: 1 / four_dim) */
+  double omega_m;
+  double z0;
+  /* extensions */
+  double rcut_over_rs; /* <= 0: no cutoff, all 27 neighbour cells (reference) */
+  int assign;          /* TPM_ASSIGN_*; default cloud4 */
+  int deconv_order;    /* sinc^-p deconvolution; 0: assignment order (4/2/3) */
+  int sort_mode;       /* TPM_SORT_*; default PARITY */
+  int kahan;           /* 1: compensated per-target PP sums (default 1) */
+  uint64_t seed;       /* synthetic-input seed carried for drivers */
+} tpm_options;
+
+typedef struct tpm_ctx tpm_ctx;
+
+/* Per-stage device times of the last calls, milliseconds (CUDA events). */
+typedef struct tpm_stage_times {
+  float sort_ms;
+  float deposit_ms;
+  float fft_forward_ms;
+  float green_ms;
+  float fft_inverse_ms;
+  float kick_ms;
+  float drift_ms;
+  float ewald_ms;
+} tpm_stage_times;
+
+/* Device addresses of the context's particle arrays (current order). */
+typedef struct tpm_device_arrays {
+  uint32_t* x;
+  uint32_t* y;
+  uint32_t* z;
+  float* vx;
+  float* vy;
+  float* vz;
+  int8_t* rung;
+  float* gx;
+  float* gy;
+  float* gz;
+  float* pot;
+  int32_t* cell_begin; /* chain_dim^3 + 1 offsets, cells keyed (z*C + y)*C + x */
+  float* phi;          /* four_dim^3 potential, x-major, z fastest */
+  int64_t n;
+} tpm_device_arrays;
+
+const char* tpm_error_string(int status);
+/* Message of the last failing call in this thread (never NULL). */
+const char* tpm_last_error_message(void);
+
+/* process_options (src/options.cpp:37-118) for the given sizes: derives
+ * four_dim = parts_dim / parts_o_four, chain_dim = parts_dim / parts_o_chain,
+ * rs = 1 / four_dim, GM = 1, hsoft = 2 / 25 / parts_dim, eta = 0.2 / sqrt 2
+ * and the cosmology constants.  Returns TPM_ERR_INVALID where the reference
+ * aborts (parts_dim not a multiple of parts_o_four * four_o_chain). */
+int tpm_options_init(tpm_options* opts, int parts_dim, int parts_o_four, int four_o_chain);
+
+/* Parses the reference's command line (--parts_dim, --parts_o_four,
+ * --four_o_chain, --box_size, --test, --config_file; src/options.cpp:47-55)
+ * plus this library's extensions (--four_dim, --chain_dim, --rs_cells,
+ * --rcut_over_rs, --assign=cloud4|cic|tsc, --sort=parity|fast, --kahan,
+ * --hsoft, --seed) into opts.  Unknown flags are TPM_ERR_INVALID. */
+int tpm_options_parse(tpm_options* opts, int argc, const char* const* argv);
+
+/* Creates a context for up to `capacity` particles on the current CUDA
+ * device.  Allocates all device memory up front (the reference allocates and
+ * frees per kick call, src/kick_pme.cu:67-107,616). */
+int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out);
+int tpm_ctx_destroy(tpm_ctx* ctx);
+int tpm_ctx_options(const tpm_ctx* ctx, tpm_options* out);
+/* Device bytes held by the context. */
+int tpm_ctx_device_bytes(const tpm_ctx* ctx, int64_t* bytes);
+/* Bytes a context for (opts, capacity) would hold, without allocating. */
+int tpm_plan_device_bytes(const tpm_options* opts, int64_t capacity, int64_t* bytes);
+
+/* Host SoA in/out (src/particles.cpp:6-12; particles_pos/vel/rung,
+ * tigerpm/particles.hpp:69-80).  Any of vx..rung may be NULL on set (zeros). */
+int tpm_set_particles(tpm_ctx* ctx, int64_t n, const uint32_t* x, const uint32_t* y,
+                      const uint32_t* z, const float* vx, const float* vy, const float* vz,
+                      const int8_t* rung);
+/* Same from device memory (pointers on the context's device). */
+int tpm_set_particles_device(tpm_ctx* ctx, int64_t n, const uint32_t* x, const uint32_t* y,
+                             const uint32_t* z, const float* vx, const float* vy,
+                             const float* vz, const int8_t* rung);
+/* Any output may be NULL. */
+int tpm_get_particles(tpm_ctx* ctx, uint32_t* x, uint32_t* y, uint32_t* z, float* vx,
+                      float* vy, float* vz, int8_t* rung);
+/* FORCE_TEST outputs particles_G / particles_P (src/particles.cpp:9-12). */
+int tpm_get_forces(tpm_ctx* ctx, float* gx, float* gy, float* gz, float* pot);
+int tpm_get_device_arrays(tpm_ctx* ctx, tpm_device_arrays* out);
+int tpm_num_particles(const tpm_ctx* ctx, int64_t* n);
+
+/* chainmesh_create (src/chainmesh.cpp:139-161; tigerpm/chainmesh.hpp:13):
+ * sorts the particles into chain cells on the device, permuting positions,
+ * velocities and rungs. */
+int tpm_chainmesh_create(tpm_ctx* ctx);
+/* chainmesh_get (src/chainmesh.cpp:48-51; tigerpm/chainmesh.hpp:17):
+ * {pbegin, pend} of cell ijk = (x, y, z); indices outside [0, C) wrap
+ * periodically (the reference's ghost cells hold the same particles). */
+int tpm_chainmesh_get(tpm_ctx* ctx, const int ijk[3], int32_t* pbegin, int32_t* pend);
+/* All C^3 + 1 cell offsets, keyed (z*C + y)*C + x. */
+int tpm_chainmesh_offsets(tpm_ctx* ctx, int32_t* offsets);
+/* chainmesh_interior_box (src/chainmesh.cpp:163-166): {b0,b1,b2,e0,e1,e2}. */
+int tpm_chainmesh_interior_box(const tpm_ctx* ctx, int box[6]);
+
+/* gravity_long_compute (src/gravity_long.cpp:36-48): deposit, r2c FFT,
+ * Green's function, c2r FFT; the potential stays on the device. */
+int tpm_gravity_long_compute(tpm_ctx* ctx, int type);
+/* gravity_long_get_phi (src/gravity_long.cpp:23-34): the potential over box
+ * {b0,b1,b2,e0,e1,e2} (any integer box; indices wrap periodically), written
+ * x-major / z fastest as range<int>::index orders it (tigerpm/range.hpp:149-165). */
+int tpm_gravity_long_get_phi(tpm_ctx* ctx, const int box[6], float* out);
+/* gravity_long_get_phi_box (src/gravity_long.cpp:19-21): the PHI_BW-padded
+ * source box of this rank. */
+int tpm_gravity_long_get_phi_box(const tpm_ctx* ctx, int box[6]);
+/* gravity_long_force_at (src/gravity_long.cpp:52-125): the 4-point cubic
+ * interpolation of phi and its gradient at n positions (double, box units),
+ * evaluated on the device. */
+int tpm_gravity_long_force_at(tpm_ctx* ctx, int64_t n, const double* pos_xyz, float* phi,
+                              float* g_xyz);
+
+/* kick_pme (src/kick_pme.cu:390-621; tigerpm/kick_pme.hpp:15): for the
+ * sink cells in box {b0,b1,b2,e0,e1,e2} (NULL: the interior box), kicks every
+ * particle with rung >= min_rung: quintic interpolation of the long-range
+ * force, erfc-split PP sum over the 27 neighbour cells, half-kicks and new
+ * rung.  Needs tpm_chainmesh_create and tpm_gravity_long_compute first.
+ * Returns TPM_ERR_RUNG if some new rung fell outside [0, 32) (clamped, the
+ * reference asserts there). */
+int tpm_kick_pme(tpm_ctx* ctx, const int* box, int min_rung, double scale, double t0,
+                 int first_call);
+
+/* Fixed-point drift (no reference counterpart): x += trunc(v * dt * 2^32)
+ * modulo 2^32 per coordinate. */
+int tpm_drift(tpm_ctx* ctx, double dt);
+
+/* gravity_short_ewald_call_kernel (src/gravity_short.cu:10-91;
+ * tigerpm/gravity_short.hpp:25-26): FP64 periodic Ewald potential and force
+ * at ns sink positions from all particles of the context.  method 0 follows
+ * the reference's sum (alpha = 2, images |n| <= 4 with r < 2.6, |h|^2 <= 8);
+ * method 1 uses alpha = 6 with precomputed structure factors (same limit to
+ * ~1e-10 relative, much faster at large n).  Near pairs (r <= hsoft) take
+ * the softened kernel as in the reference. */
+int tpm_gravity_short_ewald(tpm_ctx* ctx, int64_t ns, const uint32_t* sx, const uint32_t* sy,
+                            const uint32_t* sz, int method, double* phi, double* gx,
+                            double* gy, double* gz);
+/* Same with sinks given as particle indices in the context's current order. */
+int tpm_ewald_fp64(tpm_ctx* ctx, int64_t ns, const int64_t* sample_idx, int method,
+                   double* phi, double* gx, double* gy, double* gz);
+
+/* Stage times of the most recent calls on this context. */
+int tpm_get_stage_times(tpm_ctx* ctx, tpm_stage_times* out);
+/* Number of this library's kernel launches issued on the context so far. */
+int tpm_get_launch_count(const tpm_ctx* ctx, int64_t* count);
+/* Blocks until all work queued on the context is done. */
+int tpm_synchronize(tpm_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TPM_H_ */

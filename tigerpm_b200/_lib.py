@@ -1,0 +1,128 @@
+"""ctypes binding of the C ABI in include/tpm.h (libtigerpm_b200.so).
+
+The shared library is built in-tree by tigerpm_b200/build.py.  Loading fails
+loudly when it is missing: there is no Python or CPU fallback for any entry
+point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtigerpm_b200.so")
+
+TPM_OK = 0
+TPM_ERR_INVALID = -1
+TPM_ERR_NOMEM = -2
+TPM_ERR_CUDA = -3
+TPM_ERR_CUFFT = -4
+TPM_ERR_STATE = -5
+TPM_ERR_RUNG = -6
+TPM_ERR_CAPACITY = -7
+TPM_ERR_BUDGET = -8
+TPM_ERR_TIMEOUT = -9
+TPM_ERR_NOEXT = -10
+
+GRAVITY_LONG_PM = 0
+GRAVITY_LONG_PME = 1
+ASSIGN = {"cloud4": 0, "cic": 1, "tsc": 2}
+SORT = {"parity": 0, "fast": 1}
+
+
+class Options(C.Structure):
+    """struct tpm_options: the reference's struct options (tigerpm/options.hpp:6-27)
+    followed by this library's extensions."""
+    _fields_ = [
+        ("four_dim", C.c_int), ("chain_dim", C.c_int), ("parts_dim", C.c_int),
+        ("parts_o_four", C.c_int), ("parts_o_chain", C.c_int), ("four_o_chain", C.c_int),
+        ("eta", C.c_double), ("sigma8", C.c_double), ("code_to_cm", C.c_double),
+        ("hubble", C.c_double), ("GM", C.c_double), ("hsoft", C.c_double),
+        ("box_size", C.c_double), ("rs", C.c_double), ("omega_m", C.c_double),
+        ("z0", C.c_double),
+        ("rcut_over_rs", C.c_double), ("assign", C.c_int), ("deconv_order", C.c_int),
+        ("sort_mode", C.c_int), ("kahan", C.c_int), ("seed", C.c_uint64),
+    ]
+
+
+class StageTimes(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("sort_ms", "deposit_ms", "fft_forward_ms", "green_ms",
+                                         "fft_inverse_ms", "kick_ms", "drift_ms", "ewald_ms")]
+
+
+class DeviceArrays(C.Structure):
+    _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p), ("vx", C.c_void_p),
+                ("vy", C.c_void_p), ("vz", C.c_void_p), ("rung", C.c_void_p), ("gx", C.c_void_p),
+                ("gy", C.c_void_p), ("gz", C.c_void_p), ("pot", C.c_void_p),
+                ("cell_begin", C.c_void_p), ("phi", C.c_void_p), ("n", C.c_int64)]
+
+
+# (name, restype, argtypes) of every exported function in include/tpm.h
+_P = C.c_void_p
+_I = C.c_int
+_I64 = C.c_int64
+_D = C.c_double
+SIGNATURES = [
+    ("tpm_error_string", C.c_char_p, [_I]),
+    ("tpm_last_error_message", C.c_char_p, []),
+    ("tpm_options_init", _I, [C.POINTER(Options), _I, _I, _I]),
+    ("tpm_options_parse", _I, [C.POINTER(Options), _I, C.POINTER(C.c_char_p)]),
+    ("tpm_ctx_create", _I, [C.POINTER(Options), _I64, C.POINTER(_P)]),
+    ("tpm_ctx_destroy", _I, [_P]),
+    ("tpm_ctx_options", _I, [_P, C.POINTER(Options)]),
+    ("tpm_ctx_device_bytes", _I, [_P, C.POINTER(_I64)]),
+    ("tpm_plan_device_bytes", _I, [C.POINTER(Options), _I64, C.POINTER(_I64)]),
+    ("tpm_set_particles", _I, [_P, _I64, _P, _P, _P, _P, _P, _P, _P]),
+    ("tpm_set_particles_device", _I, [_P, _I64, _P, _P, _P, _P, _P, _P, _P]),
+    ("tpm_get_particles", _I, [_P, _P, _P, _P, _P, _P, _P, _P]),
+    ("tpm_get_forces", _I, [_P, _P, _P, _P, _P]),
+    ("tpm_get_device_arrays", _I, [_P, C.POINTER(DeviceArrays)]),
+    ("tpm_num_particles", _I, [_P, C.POINTER(_I64)]),
+    ("tpm_chainmesh_create", _I, [_P]),
+    ("tpm_chainmesh_get", _I, [_P, _P, _P, _P]),
+    ("tpm_chainmesh_offsets", _I, [_P, _P]),
+    ("tpm_chainmesh_interior_box", _I, [_P, _P]),
+    ("tpm_gravity_long_compute", _I, [_P, _I]),
+    ("tpm_gravity_long_get_phi", _I, [_P, _P, _P]),
+    ("tpm_gravity_long_get_phi_box", _I, [_P, _P]),
+    ("tpm_gravity_long_force_at", _I, [_P, _I64, _P, _P, _P]),
+    ("tpm_kick_pme", _I, [_P, _P, _I, _D, _D, _I]),
+    ("tpm_drift", _I, [_P, _D]),
+    ("tpm_gravity_short_ewald", _I, [_P, _I64, _P, _P, _P, _I, _P, _P, _P, _P]),
+    ("tpm_ewald_fp64", _I, [_P, _I64, _P, _I, _P, _P, _P, _P]),
+    ("tpm_get_stage_times", _I, [_P, C.POINTER(StageTimes)]),
+    ("tpm_get_launch_count", _I, [_P, C.POINTER(_I64)]),
+    ("tpm_synchronize", _I, [_P]),
+]
+
+_LIB = None
+
+
+class TPMError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: {msg} (status {status})")
+        self.status = status
+
+
+def load():
+    """Load libtigerpm_b200.so; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run tigerpm_b200/build.py (nvcc, sm_100a)")
+    lib = C.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def check(status: int, where: str) -> int:
+    if status != TPM_OK:
+        lib = load()
+        msg = lib.tpm_last_error_message().decode()
+        raise TPMError(status, where, msg)
+    return status

@@ -1,0 +1,308 @@
+"""Host-side mirror of the reference's PME-kick interface over the C ABI.
+
+The reference exposes free C++ functions over global particle state
+(tigerpm/kick_pme.hpp, chainmesh.hpp, gravity_long.hpp, gravity_short.hpp,
+options.hpp).  `TigerPM` keeps one periodic box on the device and offers the
+same operations under the same names, with the same argument meaning:
+
+    chainmesh_create / chainmesh_get / chainmesh_interior_box
+    gravity_long_compute / gravity_long_get_phi / gravity_long_get_phi_box /
+        gravity_long_force_at
+    kick_pme / kick_pme_begin / kick_pme_end
+    gravity_short_ewald_call_kernel / gravity_short_ewald_compare
+    drift (no reference counterpart)
+
+Every call goes to libtigerpm_b200.so; failures raise TPMError carrying the
+library's status and message (the reference prints and continues or aborts).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import GRAVITY_LONG_PM, GRAVITY_LONG_PME, Options, TPMError, check  # noqa: F401
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class Range:
+    """range<int> (tigerpm/range.hpp): half-open integer box, index() with z fastest."""
+    begin: tuple
+    end: tuple
+
+    def volume(self) -> int:
+        v = 1
+        for b, e in zip(self.begin, self.end):
+            if e < b:
+                return 0
+            v *= e - b
+        return v
+
+    def pad(self, dx: int = 1) -> "Range":
+        return Range(tuple(b - dx for b in self.begin), tuple(e + dx for e in self.end))
+
+    def shape(self):
+        return tuple(e - b for b, e in zip(self.begin, self.end))
+
+    def as_array(self):
+        return (C.c_int * 6)(*self.begin, *self.end)
+
+
+def options_for(parts_dim: int, parts_o_four: int = 3, four_o_chain: int = 5) -> Options:
+    """process_options's derived values for the given sizes (src/options.cpp:81-96)."""
+    lib = _lib.load()
+    o = Options()
+    check(lib.tpm_options_init(C.byref(o), parts_dim, parts_o_four, four_o_chain), "options_init")
+    return o
+
+
+def process_options(argv) -> Options:
+    """Parse the reference's flags (--parts_dim, --parts_o_four, --four_o_chain,
+    --box_size, --test, --config_file) plus the extensions listed in tpm.h."""
+    lib = _lib.load()
+    o = Options()
+    arr = (C.c_char_p * len(argv))(*[a.encode() for a in argv])
+    check(lib.tpm_options_parse(C.byref(o), len(argv), arr), "options_parse")
+    return o
+
+
+def make_options(n_side: int, grid: int, chain: int | None = None, rs_cells: float = 1.0,
+                 rcut_over_rs: float = 0.0, assign: str = "cloud4", sort: str = "parity",
+                 kahan: bool = True, GM: float = 1.0) -> Options:
+    """Options for a box of n_side^3 particles on a grid^3 mesh.  chain=None
+    picks the largest chain mesh whose cells are at least the cutoff wide
+    (or rcut = 4.5 rs wide when there is no cutoff)."""
+    o = options_for(n_side, 1, 1)
+    o.four_dim = grid
+    o.parts_o_four = 1
+    o.rs = rs_cells / grid
+    width = (rcut_over_rs if rcut_over_rs > 0 else 4.5) * rs_cells
+    o.chain_dim = chain if chain is not None else max(3, int(grid / width))
+    o.four_o_chain = max(1, grid // o.chain_dim)
+    o.parts_o_chain = o.four_o_chain
+    o.rcut_over_rs = rcut_over_rs
+    o.assign = _lib.ASSIGN[assign]
+    o.sort_mode = _lib.SORT[sort]
+    o.kahan = 1 if kahan else 0
+    o.GM = GM
+    return o
+
+
+def force_errors(g_test: np.ndarray, g_ref: np.ndarray, p_test=None, p_ref=None) -> dict:
+    """gravity_short_ewald_compare's metrics (src/gravity_short.cpp:53-79):
+    magnitude RMS sqrt(sum(|g1|-|g2|)^2 / sum|g2|^2), the reference's
+    "max" sum||g1|-|g2|| / sqrt(sum|g2|^2), the same for phi, plus the vector
+    RMS sqrt(sum|g1-g2|^2 / sum|g2|^2)."""
+    g1 = np.asarray(g_test, np.float64)
+    g2 = np.asarray(g_ref, np.float64)
+    m1 = np.linalg.norm(g1, axis=1)
+    m2 = np.linalg.norm(g2, axis=1)
+    norm = float(np.sum(m2 * m2))
+    out = {
+        "force_rms_vector": math.sqrt(float(np.sum((g1 - g2) ** 2)) / norm),
+        "force_rms": math.sqrt(float(np.sum((m1 - m2) ** 2)) / norm),
+        "force_max": float(np.sum(np.abs(m1 - m2))) / math.sqrt(norm),
+    }
+    if p_test is not None and p_ref is not None:
+        f1 = np.asarray(p_test, np.float64)
+        f2 = np.asarray(p_ref, np.float64)
+        pn = float(np.sum(f2 * f2))
+        out["phi_rms"] = math.sqrt(float(np.sum((f1 - f2) ** 2)) / pn)
+        out["phi_max"] = float(np.sum(np.abs(f1 - f2))) / math.sqrt(pn)
+    return out
+
+
+class TigerPM:
+    """One periodic box resident on the current CUDA device."""
+
+    def __init__(self, opts: Options, capacity: int):
+        self.lib = _lib.load()
+        self.opts = opts
+        h = C.c_void_p()
+        check(self.lib.tpm_ctx_create(C.byref(opts), int(capacity), C.byref(h)), "ctx_create")
+        self.h = h
+        self.capacity = int(capacity)
+        self.n = 0
+
+    def close(self):
+        if self.h:
+            self.lib.tpm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------ particles
+    def set_particles(self, ps) -> None:
+        """particles_X/U/R <- ps (host arrays)."""
+        x, y, z, vx, vy, vz, r = (np.ascontiguousarray(a) for a in
+                                  (ps.x, ps.y, ps.z, ps.vx, ps.vy, ps.vz, ps.rung))
+        assert x.dtype == np.uint32 and vx.dtype == np.float32 and r.dtype == np.int8
+        check(self.lib.tpm_set_particles(self.h, x.size, _ptr(x), _ptr(y), _ptr(z), _ptr(vx), _ptr(vy),
+                                         _ptr(vz), _ptr(r)), "set_particles")
+        self.n = int(x.size)
+
+    def set_particles_device(self, n: int, ptrs) -> None:
+        """From device pointers (x, y, z, vx, vy, vz, rung) as ints."""
+        check(self.lib.tpm_set_particles_device(self.h, int(n), *[C.c_void_p(p) for p in ptrs]),
+              "set_particles_device")
+        self.n = int(n)
+
+    def get_particles(self):
+        n = self.n
+        x = np.empty(n, np.uint32)
+        y = np.empty(n, np.uint32)
+        z = np.empty(n, np.uint32)
+        vx = np.empty(n, np.float32)
+        vy = np.empty(n, np.float32)
+        vz = np.empty(n, np.float32)
+        r = np.empty(n, np.int8)
+        check(self.lib.tpm_get_particles(self.h, _ptr(x), _ptr(y), _ptr(z), _ptr(vx), _ptr(vy), _ptr(vz),
+                                         _ptr(r)), "get_particles")
+        return x, y, z, vx, vy, vz, r
+
+    def get_forces(self):
+        """particles_G / particles_P of the last kick (FORCE_TEST)."""
+        n = self.n
+        g = [np.empty(n, np.float32) for _ in range(4)]
+        check(self.lib.tpm_get_forces(self.h, *[_ptr(a) for a in g]), "get_forces")
+        return g[0], g[1], g[2], g[3]
+
+    def device_arrays(self) -> _lib.DeviceArrays:
+        d = _lib.DeviceArrays()
+        check(self.lib.tpm_get_device_arrays(self.h, C.byref(d)), "get_device_arrays")
+        return d
+
+    # ----------------------------------------------------------- chain mesh
+    def chainmesh_create(self) -> None:
+        check(self.lib.tpm_chainmesh_create(self.h), "chainmesh_create")
+
+    def chainmesh_get(self, ijk):
+        b = C.c_int32()
+        e = C.c_int32()
+        arr = (C.c_int * 3)(*ijk)
+        check(self.lib.tpm_chainmesh_get(self.h, arr, C.byref(b), C.byref(e)), "chainmesh_get")
+        return int(b.value), int(e.value)
+
+    def chainmesh_offsets(self) -> np.ndarray:
+        c = self.opts.chain_dim
+        out = np.empty(c ** 3 + 1, np.int32)
+        check(self.lib.tpm_chainmesh_offsets(self.h, _ptr(out)), "chainmesh_offsets")
+        return out
+
+    def chainmesh_interior_box(self) -> Range:
+        b = (C.c_int * 6)()
+        check(self.lib.tpm_chainmesh_interior_box(self.h, b), "chainmesh_interior_box")
+        return Range(tuple(b[0:3]), tuple(b[3:6]))
+
+    # ----------------------------------------------------------- long range
+    def gravity_long_compute(self, type: int = GRAVITY_LONG_PM) -> None:
+        check(self.lib.tpm_gravity_long_compute(self.h, int(type)), "gravity_long_compute")
+
+    def gravity_long_get_phi(self, box: Range) -> np.ndarray:
+        out = np.empty(box.volume(), np.float32)
+        check(self.lib.tpm_gravity_long_get_phi(self.h, box.as_array(), _ptr(out)), "gravity_long_get_phi")
+        return out.reshape(box.shape())
+
+    def gravity_long_get_phi_box(self) -> Range:
+        b = (C.c_int * 6)()
+        check(self.lib.tpm_gravity_long_get_phi_box(self.h, b), "gravity_long_get_phi_box")
+        return Range(tuple(b[0:3]), tuple(b[3:6]))
+
+    def gravity_long_force_at(self, pos: np.ndarray):
+        """pos: (n, 3) float64 box units -> (phi[n], g[n, 3])."""
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+        n = pos.shape[0]
+        phi = np.empty(n, np.float32)
+        g = np.empty((n, 3), np.float32)
+        check(self.lib.tpm_gravity_long_force_at(self.h, n, _ptr(pos), _ptr(phi), _ptr(g)),
+              "gravity_long_force_at")
+        return phi, g
+
+    # ----------------------------------------------------------------- kick
+    def kick_pme(self, box: Range | None, min_rung: int, scale: float, t0: float, first_call: bool) -> None:
+        arr = box.as_array() if box is not None else None
+        check(self.lib.tpm_kick_pme(self.h, arr, int(min_rung), float(scale), float(t0),
+                                    1 if first_call else 0), "kick_pme")
+
+    def kick_pme_begin(self, min_rung: int, scale: float, t0: float, first_call: bool) -> None:
+        """kick_pme over chainmesh_interior_box() (src/kick_pme.cpp:9-18)."""
+        self.kick_pme(self.chainmesh_interior_box(), min_rung, scale, t0, first_call)
+
+    def kick_pme_end(self) -> None:
+        """Drops ghost particles in the reference (src/kick_pme.cpp:20-29); the
+        device mesh has no ghosts, so this only waits for the kick."""
+        check(self.lib.tpm_synchronize(self.h), "kick_pme_end")
+
+    def drift(self, dt: float) -> None:
+        check(self.lib.tpm_drift(self.h, float(dt)), "drift")
+
+    # ---------------------------------------------------------------- Ewald
+    def gravity_short_ewald_call_kernel(self, sinkx, sinky, sinkz, method: int = 1):
+        """FP64 Ewald at the sink positions from all particles of the box:
+        returns (phi, (gx, gy, gz)) like src/gravity_short.cu:10-91."""
+        sx = np.ascontiguousarray(sinkx, np.uint32)
+        sy = np.ascontiguousarray(sinky, np.uint32)
+        sz = np.ascontiguousarray(sinkz, np.uint32)
+        ns = sx.size
+        phi = np.empty(ns)
+        g = [np.empty(ns) for _ in range(3)]
+        check(self.lib.tpm_gravity_short_ewald(self.h, ns, _ptr(sx), _ptr(sy), _ptr(sz), int(method), _ptr(phi),
+                                               *[_ptr(a) for a in g]), "gravity_short_ewald")
+        return phi, tuple(g)
+
+    def ewald_samples(self, idx: np.ndarray, method: int = 1):
+        idx = np.ascontiguousarray(idx, np.int64)
+        ns = idx.size
+        phi = np.empty(ns)
+        g = [np.empty(ns) for _ in range(3)]
+        check(self.lib.tpm_ewald_fp64(self.h, ns, _ptr(idx), int(method), _ptr(phi), *[_ptr(a) for a in g]),
+              "ewald_fp64")
+        return phi, np.stack(g, axis=1)
+
+    def gravity_short_ewald_compare(self, nsamples: int, seed: int = 1, method: int = 1) -> dict:
+        """Errors of the last kick's forces against the FP64 Ewald sum on
+        nsamples distinct particles (src/gravity_short.cpp:35-82)."""
+        from .workloads import sample_indices
+        idx = sample_indices(self.n, nsamples, seed)
+        gx, gy, gz, pot = self.get_forces()
+        phi, g = self.ewald_samples(idx, method)
+        gk = np.stack([gx[idx], gy[idx], gz[idx]], axis=1)
+        out = force_errors(gk, g, pot[idx], phi)
+        out["samples"] = int(idx.size)
+        return out
+
+    # -------------------------------------------------------------- metrics
+    def stage_times(self) -> dict:
+        t = _lib.StageTimes()
+        check(self.lib.tpm_get_stage_times(self.h, C.byref(t)), "get_stage_times")
+        return {n: float(getattr(t, n)) for n, _ in _lib.StageTimes._fields_}
+
+    def launch_count(self) -> int:
+        v = C.c_int64()
+        check(self.lib.tpm_get_launch_count(self.h, C.byref(v)), "get_launch_count")
+        return int(v.value)
+
+    def device_bytes(self) -> int:
+        v = C.c_int64()
+        check(self.lib.tpm_ctx_device_bytes(self.h, C.byref(v)), "ctx_device_bytes")
+        return int(v.value)
+
+    def synchronize(self) -> None:
+        check(self.lib.tpm_synchronize(self.h), "synchronize")

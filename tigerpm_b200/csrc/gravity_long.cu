@@ -1,0 +1,374 @@
+// gravity_long.cu -- long-range PM solve on the device.
+//
+// Reference: gravity_long_compute (src/gravity_long.cpp:36-48) =
+//   compute_source (cloud4 deposit x 4 pi N, :142-199)
+//   -> fft3d_execute (unnormalised r2c, src/fft.cpp:51-67)
+//   -> apply_laplacian (-1/k^2 * exp(-k^2 rs^2) * sinc(k/2)^-4, :201-245)
+//   -> fft3d_inv_execute (1/N^3 overall, src/fft.cpp:69-84,468,512)
+//   -> get_phi (:247-256).
+//
+// Device design:
+//  * deposit: "owner computes" mesh tiles.  One block owns a T^3 tile of the
+//    grid, reads the particles of the chain cells whose assignment stencils
+//    can reach it (particles are already in chain-cell order), and
+//    accumulates the weights in shared memory as 40-bit fixed-point int64.
+//    Integer addition is associative, so the grid is bit-for-bit
+//    reproducible whatever the thread order; each grid point is written once,
+//    with no global atomics and no zeroing pass.
+//  * FFT: cuFFT r2c / c2r (the library the project allows here), timed as
+//    its own stages.
+//  * Green's function: exp(-k^2 rs^2) * sinc(k/2)^-p factorises per axis, so
+//    a per-index table (built in FP64 on the host) and k^2 = kx^2+ky^2+kz^2
+//    give G on the fly: one read + one write of the complex grid.
+#include "tpm_internal.cuh"
+
+#include <cmath>
+
+namespace tpm {
+namespace {
+
+// Per-axis assignment weights from the exact fixed-point split of X*N into
+// cell index I and fraction f (raw * N = I * 2^32 + frac).  Returns the first
+// stencil index (unwrapped).
+//  cloud4 (the reference): points I-1..I+2, cubic B-spline of the distance
+//    (src/gravity_long.cpp:127-138,176-181: I_ref = int(XN + 2) - 3 = I - 1);
+//  CIC: points I, I+1; TSC: points I0-1..I0+1 with I0 = round(XN).
+template <int ASSIGN>
+__device__ __forceinline__ int stencil(uint32_t raw, int N, float* w) {
+  const uint64_t t = (uint64_t)raw * (uint64_t)N;
+  const int I = (int)(t >> 32);
+  const float f = (float)(uint32_t)t * 2.3283064365386963e-10f;
+  if (ASSIGN == TPM_ASSIGN_CLOUD4) {
+    const float g = 1.0f - f;
+    const float s6 = 1.0f / 6.0f;
+    w[0] = s6 * g * g * g;
+    w[1] = s6 * (4.0f - 6.0f * f * f + 3.0f * f * f * f);
+    w[2] = s6 * (4.0f - 6.0f * g * g + 3.0f * g * g * g);
+    w[3] = s6 * f * f * f;
+    return I - 1;
+  } else if (ASSIGN == TPM_ASSIGN_CIC) {
+    w[0] = 1.0f - f;
+    w[1] = f;
+    return I;
+  } else {
+    const int up = f >= 0.5f ? 1 : 0;
+    const float d = f - (float)up;
+    w[0] = 0.5f * (0.5f - d) * (0.5f - d);
+    w[1] = 0.75f - d * d;
+    w[2] = 0.5f * (0.5f + d) * (0.5f + d);
+    return I + up - 1;
+  }
+}
+
+template <int ASSIGN>
+struct Width {
+  static constexpr int W = ASSIGN == TPM_ASSIGN_CLOUD4 ? 4 : (ASSIGN == TPM_ASSIGN_CIC ? 2 : 3);
+};
+
+struct DepositArgs {
+  const int4* __restrict__ pos4;
+  const int32_t* __restrict__ begin;
+  int C;
+  int N;
+  int ntile;     // tiles per side
+  double scale;  // 4 pi N * 2^-40
+  float* __restrict__ rho;
+};
+
+template <int T, int ASSIGN>
+__global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
+  constexpr int W = Width<ASSIGN>::W;
+  __shared__ unsigned long long acc[T * T * T];
+  const int N = a.N, C = a.C;
+  int tb = blockIdx.x;
+  const int tz = tb % a.ntile;
+  tb /= a.ntile;
+  const int ty = tb % a.ntile;
+  const int tx = tb / a.ntile;
+  const int o[3] = {tx * T, ty * T, tz * T};
+  int ext[3];
+  for (int d = 0; d < 3; d++) ext[d] = min(T, N - o[d]);
+  for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) acc[i] = 0ull;
+  // chain cells whose particles can reach the tile: XN in [o-2, o+T+1)
+  int clo[3], cnt[3];
+  for (int d = 0; d < 3; d++) {
+    const int lo = (int)floor(((double)o[d] - 2.001) * C / N);
+    const int hi = (int)floor(((double)o[d] + T + 1.001) * C / N);
+    clo[d] = lo;
+    cnt[d] = min(hi - lo + 1, C);
+    if (cnt[d] == C) clo[d] = 0;
+  }
+  __syncthreads();
+  const unsigned long long one = 1ull << kDepositFracBits;
+  const float fone = (float)one;
+  for (int iz = 0; iz < cnt[2]; iz++) {
+    const int cz = wrapi(clo[2] + iz, C);
+    for (int iy = 0; iy < cnt[1]; iy++) {
+      const int cy = wrapi(clo[1] + iy, C);
+      const int64_t row = ((int64_t)cz * C + cy) * C;
+      // x cells clo..clo+cnt-1 (mod C): one or two contiguous runs
+      const int x0 = wrapi(clo[0], C);
+      const int xend = x0 + cnt[0];
+      for (int part = 0; part < 2; part++) {
+        int ca, cb;
+        if (part == 0) {
+          ca = x0;
+          cb = min(xend, C);
+        } else {
+          if (xend <= C) break;
+          ca = 0;
+          cb = xend - C;
+        }
+        const int32_t pb = __ldg(a.begin + row + ca), pe = __ldg(a.begin + row + cb);
+        for (int32_t p = pb + threadIdx.x; p < pe; p += blockDim.x) {
+          const int4 q = __ldg(a.pos4 + p);
+          float wx[4], wy[4], wz[4];
+          int r[3];
+          r[0] = stencil<ASSIGN>((uint32_t)q.x, N, wx) - o[0];
+          r[1] = stencil<ASSIGN>((uint32_t)q.y, N, wy) - o[1];
+          r[2] = stencil<ASSIGN>((uint32_t)q.z, N, wz) - o[2];
+          int li[3][4];
+          bool any = true;
+          for (int d = 0; d < 3; d++) {
+            bool hit = false;
+#pragma unroll
+            for (int k = 0; k < W; k++) {
+              int l = r[d] + k;
+              if (l < 0) l += N;
+              else if (l >= N) l -= N;
+              li[d][k] = l < ext[d] ? l : -1;
+              hit |= l < ext[d];
+            }
+            any &= hit;
+          }
+          if (!any) continue;
+#pragma unroll
+          for (int i = 0; i < W; i++) {
+            if (li[0][i] < 0) continue;
+#pragma unroll
+            for (int j = 0; j < W; j++) {
+              if (li[1][j] < 0) continue;
+              const float wxy = wx[i] * wy[j];
+#pragma unroll
+              for (int k = 0; k < W; k++) {
+                if (li[2][k] < 0) continue;
+                const long long v = __float2ll_rn(wxy * wz[k] * fone);
+                atomicAdd(&acc[(li[0][i] * T + li[1][j]) * T + li[2][k]], (unsigned long long)v);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) {
+    const int lz = i % T, ly = (i / T) % T, lx = i / (T * T);
+    if (lx < ext[0] && ly < ext[1] && lz < ext[2]) {
+      const double v = (double)(long long)acc[i] * a.scale;
+      a.rho[((int64_t)(o[0] + lx) * N + (o[1] + ly)) * N + (o[2] + lz)] = (float)v;
+    }
+  }
+}
+
+__global__ void k_green(cufftComplex* __restrict__ Y, const float* __restrict__ gtab,
+                        const float* __restrict__ k2tab, int N, int Nh, float norm) {
+  const int64_t total = (int64_t)N * N * Nh;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int i2 = (int)(i % Nh);
+    const int64_t r = i / Nh;
+    const int i1 = (int)(r % N);
+    const int i0 = (int)(r / N);
+    const float k2 = __ldg(k2tab + i0) + __ldg(k2tab + i1) + __ldg(k2tab + i2);
+    const float g = k2 > 0.0f ? -(__ldg(gtab + i0) * __ldg(gtab + i1) * __ldg(gtab + i2)) / k2 * norm : 0.0f;
+    cufftComplex y = Y[i];
+    y.x *= g;
+    y.y *= g;
+    Y[i] = y;
+  }
+}
+
+__global__ void k_get_phi(const float* __restrict__ phi, int N, int b0, int b1, int b2, int s0, int s1,
+                          int s2, float* __restrict__ out) {
+  const int64_t total = (int64_t)s0 * s1 * s2;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int i2 = (int)(i % s2);
+    const int64_t r = i / s2;
+    const int i1 = (int)(r % s1);
+    const int i0 = (int)(r / s1);
+    const int g0 = wrapi(b0 + i0, N), g1 = wrapi(b1 + i1, N), g2 = wrapi(b2 + i2, N);
+    out[i] = phi[((int64_t)g0 * N + g1) * N + g2];
+  }
+}
+
+// gravity_long_force_at (src/gravity_long.cpp:52-125): 4-point cubic
+// interpolation weights and derivatives in double, periodic grid.
+__global__ void k_force_at(const float* __restrict__ phi, int N, int64_t n, const double* __restrict__ pos,
+                           float* __restrict__ phi_out, float* __restrict__ g_out) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  double X[3], w[3][4], dw[3][4];
+  int I[3];
+  for (int d = 0; d < 3; d++) {
+    X[d] = pos[3 * p + d] * N;
+    I[d] = (int)X[d];
+    X[d] -= (double)I[d];
+    I[d] -= 1;
+    const double x1 = X[d], x2 = x1 * x1, x3 = x1 * x2;
+    w[d][0] = -0.5 * x1 + x2 - 0.5 * x3;
+    w[d][1] = 1.0 - 2.5 * x2 + 1.5 * x3;
+    w[d][2] = 0.5 * x1 + 2.0 * x2 - 1.5 * x3;
+    w[d][3] = -0.5 * x2 + 0.5 * x3;
+    dw[d][0] = -0.5 + 2.0 * x1 - 1.5 * x2;
+    dw[d][1] = -5.0 * x1 + 4.5 * x2;
+    dw[d][2] = 0.5 + 4.0 * x1 - 4.5 * x2;
+    dw[d][3] = -x1 + 1.5 * x2;
+  }
+  double g[3] = {0, 0, 0}, ph = 0;
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 4; b++)
+      for (int c = 0; c < 4; c++) {
+        const double v =
+            phi[((int64_t)wrapi(I[0] + a, N) * N + wrapi(I[1] + b, N)) * N + wrapi(I[2] + c, N)];
+        g[0] += dw[0][a] * w[1][b] * w[2][c] * v * N;
+        g[1] += w[0][a] * dw[1][b] * w[2][c] * v * N;
+        g[2] += w[0][a] * w[1][b] * dw[2][c] * v * N;
+        ph += w[0][a] * w[1][b] * w[2][c] * v;
+      }
+  phi_out[p] = (float)ph;
+  for (int d = 0; d < 3; d++) g_out[3 * p + d] = (float)(-g[d]);
+}
+
+template <int T>
+void launch_deposit_T(tpm_ctx* c, const DepositArgs& a, int blocks) {
+  switch (c->opt.assign) {
+    case TPM_ASSIGN_CIC:
+      k_deposit<T, TPM_ASSIGN_CIC><<<blocks, 256, 0, c->stream>>>(a);
+      break;
+    case TPM_ASSIGN_TSC:
+      k_deposit<T, TPM_ASSIGN_TSC><<<blocks, 256, 0, c->stream>>>(a);
+      break;
+    default:
+      k_deposit<T, TPM_ASSIGN_CLOUD4><<<blocks, 256, 0, c->stream>>>(a);
+      break;
+  }
+}
+
+}  // namespace
+
+int mesh_init(tpm_ctx* c) {
+  const int N = c->N;
+  const int Nh = N / 2 + 1;
+  // Per-index factor exp(-k^2 rs^2) * sinc(k/2)^-p and k^2, k = 2 pi i / N
+  // with i >= N/2 folded negative (src/gravity_long.cpp:214-239), built in FP64.
+  std::vector<float> g(N), g_pm(N), k2(N);
+  const double rs_cells = c->rs_box * N;
+  int p = c->opt.deconv_order;
+  if (p <= 0) p = c->opt.assign == TPM_ASSIGN_CIC ? 2 : (c->opt.assign == TPM_ASSIGN_TSC ? 3 : 4);
+  for (int i = 0; i < N; i++) {
+    const double k = (i < N / 2.0 ? i : i - N) * 2.0 * M_PI / N;
+    const double x = 0.5 * k;
+    const double s = x != 0.0 ? std::sin(x) / x : 1.0;
+    const double dec = std::pow(s, -p);
+    g[i] = (float)(std::exp(-k * k * rs_cells * rs_cells) * dec);
+    g_pm[i] = (float)dec;
+    k2[i] = (float)(k * k);
+  }
+  TPM_CUDA_TRY(cudaMemcpy(c->gtab, g.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+  TPM_CUDA_TRY(cudaMemcpy(c->gtab + N, g_pm.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+  TPM_CUDA_TRY(cudaMemcpy(c->k2tab, k2.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+  TPM_CUFFT_TRY(cufftPlan3d(&c->plan_r2c, N, N, N, CUFFT_R2C));
+  TPM_CUFFT_TRY(cufftPlan3d(&c->plan_c2r, N, N, N, CUFFT_C2R));
+  TPM_CUFFT_TRY(cufftSetStream(c->plan_r2c, c->stream));
+  TPM_CUFFT_TRY(cufftSetStream(c->plan_c2r, c->stream));
+  c->plans = true;
+  c->deposit_tile = N >= 256 ? 16 : 8;
+  (void)Nh;
+  return TPM_OK;
+}
+
+int gravity_long(tpm_ctx* c, int type) {
+  if (!c->sorted) return fail(TPM_ERR_STATE, "gravity_long_compute needs chainmesh_create first");
+  const int N = c->N;
+  const int Nh = N / 2 + 1;
+  cudaStream_t s = c->stream;
+  stage_begin(c, kStDeposit);
+  DepositArgs a;
+  a.pos4 = c->pos4;
+  a.begin = c->cell_begin;
+  a.C = c->C;
+  a.N = N;
+  a.scale = 4.0 * M_PI * N * std::ldexp(1.0, -kDepositFracBits);
+  a.rho = c->rho;
+  if (c->deposit_tile == 16) {
+    a.ntile = ceil_div(N, 16);
+    launch_deposit_T<16>(c, a, a.ntile * a.ntile * a.ntile);
+  } else {
+    a.ntile = ceil_div(N, 8);
+    launch_deposit_T<8>(c, a, a.ntile * a.ntile * a.ntile);
+  }
+  c->launches++;
+  TPM_CUDA_TRY(cudaGetLastError());
+  stage_end(c, kStDeposit);
+  stage_begin(c, kStFftF);
+  TPM_CUFFT_TRY(cufftExecR2C(c->plan_r2c, c->rho, c->rhok));
+  stage_end(c, kStFftF);
+  stage_begin(c, kStGreen);
+  const int64_t total = (int64_t)N * N * Nh;
+  const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 148 * 32);
+  const float* gt = type == TPM_GRAVITY_LONG_PME ? c->gtab : c->gtab + N;
+  k_green<<<blocks, 256, 0, s>>>(c->rhok, gt, c->k2tab, N, Nh, (float)(1.0 / ((double)N * N * N)));
+  c->launches++;
+  TPM_CUDA_TRY(cudaGetLastError());
+  stage_end(c, kStGreen);
+  stage_begin(c, kStFftI);
+  TPM_CUFFT_TRY(cufftExecC2R(c->plan_c2r, c->rhok, c->phi));
+  stage_end(c, kStFftI);
+  c->have_phi = true;
+  return TPM_OK;
+}
+
+int gravity_long_get_phi(tpm_ctx* c, const int box[6], float* out) {
+  if (!c->have_phi) return fail(TPM_ERR_STATE, "gravity_long_get_phi needs gravity_long_compute first");
+  const int s0 = box[3] - box[0], s1 = box[4] - box[1], s2 = box[5] - box[2];
+  if (s0 < 0 || s1 < 0 || s2 < 0) return fail(TPM_ERR_INVALID, "negative box extent");
+  const int64_t total = (int64_t)s0 * s1 * s2;
+  if (total == 0) return TPM_OK;
+  float* d = nullptr;
+  TPM_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(float) * total, c->stream));
+  k_get_phi<<<(int)std::min<int64_t>(ceil_div(total, 256), 148 * 16), 256, 0, c->stream>>>(
+      c->phi, c->N, box[0], box[1], box[2], s0, s1, s2, d);
+  c->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, sizeof(float) * total, cudaMemcpyDeviceToHost, c->stream);
+  cudaFreeAsync(d, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return fail(TPM_ERR_CUDA, std::string("get_phi: ") + cudaGetErrorString(e));
+  return TPM_OK;
+}
+
+int gravity_long_force_at(tpm_ctx* c, int64_t n, const double* pos, float* phi_out, float* g_out) {
+  if (!c->have_phi) return fail(TPM_ERR_STATE, "gravity_long_force_at needs gravity_long_compute first");
+  if (n <= 0) return TPM_OK;
+  double* dpos = nullptr;
+  float* dout = nullptr;
+  TPM_CUDA_TRY(cudaMallocAsync((void**)&dpos, sizeof(double) * 3 * n, c->stream));
+  TPM_CUDA_TRY(cudaMallocAsync((void**)&dout, sizeof(float) * 4 * n, c->stream));
+  cudaError_t e = cudaMemcpyAsync(dpos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) {
+    k_force_at<<<ceil_div(n, 128), 128, 0, c->stream>>>(c->phi, c->N, n, dpos, dout, dout + n);
+    c->launches++;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(phi_out, dout, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(g_out, dout + n, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, c->stream);
+  cudaFreeAsync(dpos, c->stream);
+  cudaFreeAsync(dout, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return fail(TPM_ERR_CUDA, std::string("force_at: ") + cudaGetErrorString(e));
+  return TPM_OK;
+}
+
+}  // namespace tpm

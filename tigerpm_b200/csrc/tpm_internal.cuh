@@ -1,0 +1,164 @@
+// tpm_internal.cuh -- context layout and shared device helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/tpm.h"
+
+namespace tpm {
+
+constexpr int kMaxRung = 32;      // MAX_RUNG, tigerpm/tigerpm.hpp:34
+constexpr int kNInterp = 6;       // NINTERP, tigerpm/tigerpm.hpp:35
+constexpr int kPhiBW = 3;         // PHI_BW, tigerpm/tigerpm.hpp:41
+constexpr int kMaxTreeDepth = 24; // 1-D bisection depth bound (C < 2^23)
+constexpr int kDepositFracBits = 40;
+
+// Error bits a kernel may raise in ctx->d_err (never a trap).
+constexpr int kErrRung = 1;
+constexpr int kErrBounds = 2;
+
+// Records a failure message for tpm_last_error_message and returns status.
+int fail(int status, const std::string& msg);
+#define TPM_CUDA_TRY(call)                                                       \
+  do {                                                                           \
+    cudaError_t e_ = (call);                                                     \
+    if (e_ != cudaSuccess)                                                       \
+      return ::tpm::fail(TPM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+#define TPM_CUFFT_TRY(call)                                                      \
+  do {                                                                           \
+    cufftResult r_ = (call);                                                     \
+    if (r_ != CUFFT_SUCCESS)                                                     \
+      return ::tpm::fail(TPM_ERR_CUFFT, std::string(#call) + " failed: " + std::to_string((int)r_)); \
+  } while (0)
+
+// One node of the 1-D bisection tree over [0, C) that the reference's chain
+// sort applies per dimension (split at lo + span/2, src/chainmesh.cpp:198).
+struct TreeNode {
+  int lo, mid, hi, pad;
+};
+
+struct StageEvents {
+  cudaEvent_t beg[8];
+  cudaEvent_t end[8];
+  bool used[8];
+};
+
+enum Stage { kStSort = 0, kStDeposit, kStFftF, kStGreen, kStFftI, kStKick, kStDrift, kStEwald };
+
+}  // namespace tpm
+
+struct tpm_ctx {
+  tpm_options opt;
+  int N = 0;  // four_dim
+  int C = 0;  // chain_dim
+  double rs_box = 0;
+  double rcut_box = 0;  // 0: none
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t cap = 0;
+  int64_t n = 0;
+  bool sorted = false;
+  bool have_phi = false;
+  bool host_cells_valid = false;
+
+  // particles, current order
+  uint32_t *x = nullptr, *y = nullptr, *z = nullptr;
+  float *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  int8_t* rung = nullptr;
+  float *gx = nullptr, *gy = nullptr, *gz = nullptr, *pot = nullptr;
+  int4* pos4 = nullptr;  // packed (x, y, z, 0) in chain order for PP staging
+
+  // sort scratch
+  uint32_t *x2 = nullptr, *y2 = nullptr, *z2 = nullptr;
+  float *vx2 = nullptr, *vy2 = nullptr, *vz2 = nullptr;
+  int8_t* rung2 = nullptr;
+  uint32_t* key = nullptr;    // cell key of the particle at each position
+  int32_t* idx = nullptr;     // original index of the particle at each position
+  int32_t* cellof = nullptr;  // final cell whose range holds each position
+  int32_t* prefix = nullptr;  // exclusive scan of the per-level flags (n + 1)
+  int32_t* slot = nullptr;    // partner positions of right-misplaced elements
+  int32_t* blocksum = nullptr;
+  int32_t* cell_count = nullptr;
+  int32_t* cell_begin = nullptr;  // C^3 + 1
+  uint32_t* thr = nullptr;        // per-dim split thresholds, C + 1
+  tpm::TreeNode* tree = nullptr;  // [C * kMaxTreeDepth]
+  int* depth1d = nullptr;         // [C]
+  int max_depth1d = 0;
+
+  // mesh
+  float* rho = nullptr;  // N^3 real grid (deposit out, r2c in)
+  cufftComplex* rhok = nullptr;
+  float* phi = nullptr;  // N^3
+  float* gtab = nullptr;   // exp(-k^2 rs^2) sinc(k/2)^-p per index, N
+  float* k2tab = nullptr;  // k^2 per index, N
+  cufftHandle plan_r2c = 0, plan_c2r = 0;
+  bool plans = false;
+  int deposit_tile = 8;
+
+  // ewald scratch
+  double* ew_buf = nullptr;
+  int64_t ew_cap = 0;
+
+  int* d_err = nullptr;
+  int64_t launches = 0;
+  int64_t device_bytes = 0;
+  tpm::StageEvents ev{};
+  std::vector<int32_t> host_cells;
+};
+
+namespace tpm {
+
+// Stage timing helpers.
+void stage_begin(tpm_ctx* c, Stage s);
+void stage_end(tpm_ctx* c, Stage s);
+
+// Kernel families (each returns TPM_OK or an error).
+int chainmesh_sort(tpm_ctx* c);
+int gravity_long(tpm_ctx* c, int type);
+int gravity_long_get_phi(tpm_ctx* c, const int box[6], float* out);
+int gravity_long_force_at(tpm_ctx* c, int64_t n, const double* pos, float* phi, float* g);
+int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0, int first_call);
+int drift(tpm_ctx* c, double dt);
+int ewald(tpm_ctx* c, int64_t ns, const uint32_t* dsx, const uint32_t* dsy, const uint32_t* dsz,
+          int method, double* phi, double* gx, double* gy, double* gz);
+int mesh_init(tpm_ctx* c);
+int sort_init(tpm_ctx* c);
+
+inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// -------------------------------------------------------------- device math
+
+// distance(a, b): int32 wrap-around difference * 2^-32
+// (tigerpm/gravity_short.hpp:20-22).
+__device__ __forceinline__ float distance32(uint32_t a, uint32_t b) {
+  return (float)(int32_t)(a - b) * 2.3283064365386963e-10f;
+}
+
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ int wrapi(int i, int n) {
+  int r = i % n;
+  return r < 0 ? r + n : r;
+}
+
+}  // namespace tpm
