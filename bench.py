@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""PME particle-kicks/s on B200 (tigerpm_b200) -- one JSON line on rank 0.
+
+A step is one whole PME kick of every particle of a box, as the reference's
+kick_pme_test runs it (src/test.cpp:182-234): restore the box's particles,
+chain-mesh sort, deposit, r2c FFT, Green's function, c2r FFT, interpolation +
+short-range PP + rung kick.  `value` times the step with the inputs already
+resident in HBM; `e2e` times the same step through the C ABI from pinned host
+buffers (H2D of the particles, D2H of the kicked particles) every step.
+
+Workloads (synthetic, seeded Philox; see tigerpm_b200/workloads.py):
+  c2-accurate  (default) 256^3 Zel'dovich particles (P(k) ~ k^-2 cut at
+               k_Nyq/2, rms displacement 0.3 particle spacings), the
+               reference's cloud4 deposit on a 512^3 mesh, r_s = 2 mesh
+               cells, cutoff 5.5 r_s: the form of the 256^3 configuration that
+               meets rms force error <= 1e-4 (TSC and the literal r_s / mesh
+               do not; see the accuracy study).
+  c2           the same particles with the configuration's literal mesh
+               parameters: 256^3 mesh, TSC, r_s = 1.25 cells, cutoff 4.5 r_s.
+  c1           64^3 uniform particles, 64^3 mesh, CIC, r_s 1.25, 4.5 r_s.
+Every run also reports the rms force error of the kick against the FP64
+Ewald sum on 4,096 sampled particles.
+
+--impl reference times the oracle (oracle/, the CPU restatement of the
+reference path; the reference itself cannot be built here) on the host
+cores on the same workload; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "c2-accurate": dict(kind="zeldovich", n_side=256, grid=512, assign="cloud4", rs_cells=2.0, rcut_over_rs=5.5,
+                        ewald_samples=4096),
+    "c2": dict(kind="zeldovich", n_side=256, grid=256, assign="tsc", rs_cells=1.25, rcut_over_rs=4.5,
+               ewald_samples=4096),
+    "c1": dict(kind="uniform", n_side=64, grid=64, assign="cic", rs_cells=1.25, rcut_over_rs=4.5,
+               ewald_samples=1000),
+}
+METRIC = "PME particle-kicks/s at rms force err<=1e-4 vs FP64 Ewald"
+FLOPS_PER_PAIR = 44.0      # in-cutoff pair, FMA = 2, MUFU = 1 (the reference's inner loop)
+FLOPS_PER_CULLED = 8.0     # candidate pair rejected by the r^2 test
+
+
+def make_particles(cfg, seed):
+    from tigerpm_b200 import workloads as W
+    if cfg["kind"] == "uniform":
+        return W.uniform(cfg["n_side"] ** 3, seed)
+    return W.zeldovich(cfg["n_side"], seed, rms_cells=0.3, grid=cfg["n_side"])
+
+
+def make_opts(cfg):
+    from tigerpm_b200.api import make_options
+    return make_options(cfg["n_side"], cfg["grid"], rs_cells=cfg["rs_cells"], rcut_over_rs=cfg["rcut_over_rs"],
+                        assign=cfg["assign"])
+
+
+def host_opts(cfg):
+    """The same option values make_opts derives, computed without the CUDA
+    library (the reference arm must not load it)."""
+    from types import SimpleNamespace
+    grid = cfg["grid"]
+    width = cfg["rcut_over_rs"] * cfg["rs_cells"]
+    return SimpleNamespace(four_dim=grid, chain_dim=max(3, int(grid / width)), rs=cfg["rs_cells"] / grid,
+                           hsoft=2.0 / 25.0 / cfg["n_side"], eta=0.2 / math.sqrt(2.0), GM=1.0,
+                           rcut_over_rs=cfg["rcut_over_rs"])
+
+
+def workload_desc(name, cfg, opts):
+    return {
+        "workload": f"{name}: {cfg['n_side']}^3 {cfg['kind']} particles, {cfg['grid']}^3 mesh {cfg['assign'].upper()}, "
+                    f"r_s={cfg['rs_cells']} cells, cutoff={cfg['rcut_over_rs']} r_s, chain mesh {opts.chain_dim}^3",
+        "particles": cfg["n_side"] ** 3, "grid": cfg["grid"], "assign": cfg["assign"], "rs_cells": cfg["rs_cells"],
+        "rcut_over_rs": cfg["rcut_over_rs"], "chain_dim": opts.chain_dim, "sort": "parity",
+        "precision": "fp32 pair terms, Kahan-compensated per-target sums",
+        "l2": "inputs larger than L2 (particles + mesh > 126 MB)",
+    }
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# -------------------------------------------------------------- GPU arm
+def gpu_arm(args, cfg, name, rank, world, dist):
+    import torch
+    from tigerpm_b200 import _lib
+    from tigerpm_b200.api import TigerPM, fp32_peak_probe
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    ps = make_particles(cfg, args.seed + rank)
+    n = ps.n
+    opts = make_opts(cfg)
+    ctx = TigerPM(opts, n)
+    ext = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    # resident inputs (pristine copy in HBM) and pinned host buffers for e2e
+    dev_in = [torch.from_numpy(a).to(dev) for a in ps.arrays()]
+    pinned_in = [torch.from_numpy(a).pin_memory() for a in ps.arrays()]
+    pinned_out = [torch.empty_like(t).pin_memory() for t in pinned_in]
+    ptr_in = [t.data_ptr() for t in dev_in]
+    lib = _lib.load()
+    import ctypes as C
+
+    def step_resident():
+        ctx.set_particles_device(n, ptr_in)
+        ctx.pme_step(0, 1.0, 1.0, True)
+
+    h_in = [C.c_void_p(t.data_ptr()) for t in pinned_in]
+    h_out = [C.c_void_p(t.data_ptr()) for t in pinned_out]
+
+    def step_e2e():
+        _lib.check(lib.tpm_set_particles(ctx.h, n, *h_in), "set_particles")
+        ctx.pme_step(0, 1.0, 1.0, True)
+        _lib.check(lib.tpm_get_particles(ctx.h, *h_out), "get_particles")
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+
+    def timed(fn, steps):
+        barrier()
+        ctx.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        for _ in range(steps):
+            fn()
+        e1.record(ext)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    for _ in range(args.warmup):
+        step_resident()
+    ctx.check_errors()
+    ctx.reset_stage_times()
+    l0 = ctx.launch_count()
+    with ClockSampler(dev.index) as clk:
+        ms = timed(step_resident, args.steps)
+    launches = (ctx.launch_count() - l0) // args.steps * args.steps
+    ctx.check_errors()
+    stages = ctx.stage_times()
+    for _ in range(max(1, args.warmup // 2)):
+        step_e2e()
+    ms_e2e = timed(step_e2e, args.steps)
+
+    total = n * world * args.steps
+    out = {
+        "value": total / (ms * 1e-3), "ms_per_step": ms / args.steps,
+        "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "particle-kicks/s",
+                "h2d_bytes_per_step": int(sum(t.numel() * t.element_size() for t in pinned_in)),
+                "d2h_bytes_per_step": int(sum(t.numel() * t.element_size() for t in pinned_out)),
+                "ms_per_step": ms_e2e / args.steps},
+        "stages_ms": {k: round(v, 4) for k, v in stages.items() if v > 0},
+        "gpu_launches": int(launches), "clocks": clk.summary(),
+    }
+    # roofline of the dominant kernel (PP: FP32-bound)
+    cand, inside = ctx.count_pairs(0)
+    flops = FLOPS_PER_PAIR * inside + FLOPS_PER_CULLED * (cand - inside)
+    kick_ms = stages["kick_ms"]
+    peak = fp32_peak_probe()
+    achieved = flops / (kick_ms * 1e-3) / 1e12
+    out["roofline"] = {"bound": "fp32", "kernel": "k_kick_pme", "achieved": round(achieved, 3),
+                       "peak": round(peak, 2), "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+                       "traffic": read_traffic(name),
+                       "peak_source": "measured FP32 FMA probe on this GPU (tpm_fp32_peak_probe)",
+                       "pairs_in_cutoff": inside, "pairs_candidate": cand,
+                       "flops_per_launch": flops, "kick_ms": round(kick_ms, 4)}
+    # accuracy of this kick vs the FP64 Ewald sum
+    if args.ewald_samples:
+        step_resident()
+        ctx.check_errors()
+        err = ctx.gravity_short_ewald_compare(min(args.ewald_samples, cfg["ewald_samples"]), seed=args.seed + 7)
+        out["accuracy"] = {k: (float(f"{v:.4e}") if isinstance(v, float) else v) for k, v in err.items()}
+    ctx.close()
+    return out
+
+
+def read_traffic(name):
+    """DRAM bytes per kick launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"kick_pme_{name}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------- CPU (oracle) arm
+def cpu_estimate(cfg, opts, ps, threads, budget_s):
+    """Seconds for one whole kick of the workload on the host cores with the
+    oracle: sort, deposit, FFT + Green + inverse FFT timed in full; the PP +
+    interpolation + kick timed on a random sample of sink cells sized to
+    ~budget_s and extrapolated by candidate-pair counts."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from tigerpm_b200 import workloads as W
+    p = O.Particles(*(np.array(a, copy=True) for a in ps.arrays()))
+    C_, N = opts.chain_dim, opts.four_dim
+    t = time.perf_counter()
+    pb, pe = O.chainmesh_sort(C_, p, nthreads=threads)
+    t_sort = time.perf_counter() - t
+    t = time.perf_counter()
+    phi = O.gravity_long(N, cfg["rs_cells"], {"cloud4": 0, "cic": 1, "tsc": 2}[cfg["assign"]], p.x, p.y, p.z,
+                         nthreads=threads)
+    t_long = time.perf_counter() - t
+    counts = (pe - pb).astype(np.int64).reshape(C_, C_, C_)
+    nb = np.zeros_like(counts)
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                nb += np.roll(counts, (dz, dy, dx), axis=(0, 1, 2))
+    cand_total = float(np.sum(counts * nb))
+    kp = O.KickParams(N=N, C=C_, rs=opts.rs, GM=opts.GM, eta=opts.eta, hsoft=opts.hsoft,
+                      rcut=opts.rcut_over_rs * opts.rs, min_rung=0, scale=1.0, t0=1.0, first_call=1, precision=0)
+    g = W.rng(12345)
+    order = g.permutation(C_ ** 3).astype(np.int32)
+    ncell = 8
+    t_pp = 0.0
+    cand_s = 0.0
+    used = 0
+    phi32 = phi.astype(np.float32)
+    while used < order.size:
+        cells = order[used:used + ncell]
+        t = time.perf_counter()
+        _, _, _, _, cnt, _ = O.kick_pme(kp, p, pb, pe, phi32, sink_cells=cells, nthreads=threads)
+        t_pp += time.perf_counter() - t
+        cand_s += float(cnt[0])
+        used += cells.size
+        if t_pp > budget_s:
+            break
+        ncell = min(ncell * 2, order.size - used)
+    t_kick = t_pp * cand_total / max(cand_s, 1.0)
+    total = t_sort + t_long + t_kick
+    sample = (f"sort + deposit + FFT/Green/iFFT timed in full; PP+interp+kick timed on {used} of {C_**3} "
+              f"sink cells ({100.0 * cand_s / cand_total:.2f}% of candidate pairs) and extrapolated by pair count")
+    return total, {"sort_s": round(t_sort, 3), "long_range_s": round(t_long, 3), "kick_s_extrapolated": round(t_kick, 3),
+                   "kick_sample_s": round(t_pp, 3)}, sample
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2-accurate", choices=sorted(CONFIGS))
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--ewald-samples", type=int, default=4096)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-named", action="store_true", help="skip the literal c2 secondary measurement")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    cfg = CONFIGS[args.config]
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        opts = host_opts(cfg)
+        ps = make_particles(cfg, args.seed)
+        th = cpu_threads()
+        times = []
+        for i in range(args.warmup + args.steps):
+            tt, parts, sample = cpu_estimate(cfg, opts, ps, th, budget_s=2.0)
+            if i >= args.warmup:
+                times.append(tt)
+        sec = statistics.mean(times)
+        v = ps.n / sec
+        line = {"metric": METRIC, "value": v, "unit": "particle-kicks/s", "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": workload_desc(args.config, cfg, opts),
+                "cpu_baseline": {"value": v, "unit": "particle-kicks/s", "cores": th, "kind": "port",
+                                 "sample": sample, "stages_s": parts},
+                "e2e": {"value": v, "unit": "particle-kicks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        import datetime
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = dist_mod
+    res = gpu_arm(args, cfg, args.config, rank, world, dist)
+    named = None
+    if args.config == "c2-accurate" and not args.no_named:
+        ncfg = CONFIGS["c2"]
+        named = gpu_arm(args, ncfg, "c2", rank, world, dist)
+    if rank == 0:
+        opts = make_opts(cfg)
+        line = {"metric": METRIC, "value": res["value"], "unit": "particle-kicks/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded Philox; Zel'dovich / uniform as configured)",
+                "config": dict(workload_desc(args.config, cfg, opts), parallelism=f"replicas x{world}"),
+                "e2e": res["e2e"], "roofline": res["roofline"], "gpu_launches": res["gpu_launches"],
+                "clocks": res["clocks"], "stages_ms": res["stages_ms"], "accuracy": res.get("accuracy")}
+        if named is not None:
+            line["named_config"] = {"config": workload_desc("c2", CONFIGS["c2"], make_opts(CONFIGS["c2"])),
+                                    "value": named["value"], "ms_per_step": named["ms_per_step"],
+                                    "e2e": named["e2e"]["value"], "accuracy": named.get("accuracy"),
+                                    "stages_ms": named["stages_ms"], "roofline_frac": named["roofline"]["frac"]}
+        if world == 1 and not args.no_cpu_baseline:
+            ps = make_particles(cfg, args.seed)
+            th = cpu_threads()
+            sec, parts, sample = cpu_estimate(cfg, opts, ps, th, budget_s=8.0)
+            line["cpu_baseline"] = {"value": ps.n / sec, "unit": "particle-kicks/s", "cores": th, "kind": "port",
+                                    "sample": sample, "stages_s": parts}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

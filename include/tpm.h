@@ -230,12 +230,35 @@ int tpm_gravity_short_ewald(tpm_ctx* ctx, int64_t ns, const uint32_t* sx, const 
 int tpm_ewald_fp64(tpm_ctx* ctx, int64_t ns, const int64_t* sample_idx, int method,
                    double* phi, double* gx, double* gy, double* gz);
 
-/* Stage times of the most recent calls on this context. */
+/* Average device time per call of each stage over the calls since the last
+ * tpm_reset_stage_times (up to the last 64 calls per stage). */
 int tpm_get_stage_times(tpm_ctx* ctx, tpm_stage_times* out);
+int tpm_reset_stage_times(tpm_ctx* ctx);
 /* Number of this library's kernel launches issued on the context so far. */
 int tpm_get_launch_count(const tpm_ctx* ctx, int64_t* count);
 /* Blocks until all work queued on the context is done. */
 int tpm_synchronize(tpm_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for event timing by callers. */
+int tpm_ctx_stream(tpm_ctx* ctx, void** stream);
+
+/* One whole PME kick without host synchronisation: chainmesh_create,
+ * gravity_long_compute(PME) and kick_pme over the interior box -- the
+ * sequence of the reference's kick_pme_test (src/test.cpp:182-234).  Kernel
+ * error flags are collected on the device; read them with tpm_check_errors. */
+int tpm_pme_step(tpm_ctx* ctx, int min_rung, double scale, double t0, int first_call);
+/* Synchronises and reports (then clears) device error flags raised since the
+ * last check: TPM_ERR_RUNG for a clamped rung, TPM_ERR_INVALID for a drift
+ * step beyond 2^31 box lengths. */
+int tpm_check_errors(tpm_ctx* ctx);
+
+/* Candidate sink-source pairs of the 27-cell neighbourhoods (active sinks,
+ * rung >= min_rung) and the pairs inside the cutoff, counted on the device. */
+int tpm_count_pairs(tpm_ctx* ctx, int min_rung, int64_t* candidates, int64_t* inside);
+
+/* Measured FP32 FMA throughput of the current device (TFLOP/s), from a
+ * dense FMA-chain kernel: the denominator for the PP kernel's roofline. */
+int tpm_fp32_peak_probe(double* tflops);
 
 #ifdef __cplusplus
 }

@@ -91,8 +91,14 @@ SIGNATURES = [
     ("tpm_gravity_short_ewald", _I, [_P, _I64, _P, _P, _P, _I, _P, _P, _P, _P]),
     ("tpm_ewald_fp64", _I, [_P, _I64, _P, _I, _P, _P, _P, _P]),
     ("tpm_get_stage_times", _I, [_P, C.POINTER(StageTimes)]),
+    ("tpm_reset_stage_times", _I, [_P]),
     ("tpm_get_launch_count", _I, [_P, C.POINTER(_I64)]),
     ("tpm_synchronize", _I, [_P]),
+    ("tpm_ctx_stream", _I, [_P, C.POINTER(_P)]),
+    ("tpm_pme_step", _I, [_P, _I, _D, _D, _I]),
+    ("tpm_check_errors", _I, [_P]),
+    ("tpm_count_pairs", _I, [_P, _I, C.POINTER(_I64), C.POINTER(_I64)]),
+    ("tpm_fp32_peak_probe", _I, [C.POINTER(_D)]),
 ]
 
 _LIB = None

@@ -294,6 +294,9 @@ class TigerPM:
         check(self.lib.tpm_get_stage_times(self.h, C.byref(t)), "get_stage_times")
         return {n: float(getattr(t, n)) for n, _ in _lib.StageTimes._fields_}
 
+    def reset_stage_times(self) -> None:
+        check(self.lib.tpm_reset_stage_times(self.h), "reset_stage_times")
+
     def launch_count(self) -> int:
         v = C.c_int64()
         check(self.lib.tpm_get_launch_count(self.h, C.byref(v)), "get_launch_count")
@@ -306,3 +309,30 @@ class TigerPM:
 
     def synchronize(self) -> None:
         check(self.lib.tpm_synchronize(self.h), "synchronize")
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        check(self.lib.tpm_ctx_stream(self.h, C.byref(p)), "ctx_stream")
+        return int(p.value or 0)
+
+    def pme_step(self, min_rung: int = 0, scale: float = 1.0, t0: float = 1.0, first_call: bool = True) -> None:
+        """chainmesh_create + gravity_long_compute(PME) + kick_pme, no host sync."""
+        check(self.lib.tpm_pme_step(self.h, int(min_rung), float(scale), float(t0), 1 if first_call else 0),
+              "pme_step")
+
+    def check_errors(self) -> None:
+        check(self.lib.tpm_check_errors(self.h), "check_errors")
+
+    def count_pairs(self, min_rung: int = 0):
+        a = C.c_int64()
+        b = C.c_int64()
+        check(self.lib.tpm_count_pairs(self.h, int(min_rung), C.byref(a), C.byref(b)), "count_pairs")
+        return int(a.value), int(b.value)
+
+
+def fp32_peak_probe() -> float:
+    """Measured FP32 FMA throughput of the current device, TFLOP/s."""
+    lib = _lib.load()
+    v = C.c_double()
+    check(lib.tpm_fp32_peak_probe(C.byref(v)), "fp32_peak_probe")
+    return float(v.value)

@@ -16,20 +16,26 @@
 //    float offsets from the sink cell centre: the int32 wrap-around
 //    difference (the reference's periodic minimum image) is taken once per
 //    source per block, so the pair loop is pure FP32 (FADD for dx).
+//  * Culling: the cell's sinks (up to 256 at a time) are ordered by a 9-bit
+//    Morton key of their position inside the cell (a deterministic bitonic
+//    sort in shared memory), so each warp holds 32 spatially compact sinks.
+//    Each warp compacts every staged source tile to the sources within the
+//    cutoff of its sinks' bounding box (ballot + popc into a per-warp index
+//    list) and evaluates only those; the exact r < rcut test stays per pair.
 //  * Pair kernel: rsqrt / rcp / ex2 approximations (MUFU) for 1/r, the A&S
 //    rational and exp(-x^2); an optional cutoff masks pairs beyond rcut.
 //  * Precision: FP32 pair terms summed in chunks of 64 sources, chunk sums
 //    added with Kahan compensation per target (kahan option).
 #include "tpm_internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 
 namespace tpm {
 namespace {
 
 constexpr int kKickThreads = 256;
-constexpr int kTile = 1024;
-constexpr int kChunk = 64;
+constexpr int kMaxStage = 4096;  // sources staged per chunk (64 KB)
 
 struct KickArgs {
   const int4* __restrict__ pos4;
@@ -102,7 +108,7 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
   float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
   for (int i = 0; i < kNInterp; i++) {
     const int64_t plane = (int64_t)wrapi(base[0] + i, N) * N * N;
-    float px = 0.f, py = 0.f, pz = 0.f, pp = 0.f;
+    float px = 0.f, py = 0.f, pz = 0.f;
 #pragma unroll
     for (int j = 0; j < kNInterp; j++) {
       float rz = 0.f, rdz = 0.f;
@@ -120,7 +126,6 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
     sy = fmaf(w[0][i], py, sy);
     sz = fmaf(w[0][i], pz, sz);
     sp = fmaf(w[0][i], px, sp);
-    (void)pp;
   }
   lx = -sx * (float)N;
   ly = -sy * (float)N;
@@ -157,8 +162,51 @@ __device__ __forceinline__ void pair(const KickArgs& a, float dx, float dy, floa
   ph -= rinv1;
 }
 
-__global__ void __launch_bounds__(kKickThreads) k_kick_pme(KickArgs a) {
-  __shared__ float4 src[kTile];
+
+// 3-bit-per-axis sub-cell index of an offset (in box units) from the cell
+// centre, interleaved into a 9-bit Morton key.
+__device__ __forceinline__ unsigned morton9(float sx, float sy, float sz, float C) {
+  unsigned q[3];
+  const float s[3] = {sx, sy, sz};
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const int v = (int)((s[d] * C + 0.5f) * 8.0f);
+    q[d] = (unsigned)min(max(v, 0), 7);
+  }
+  unsigned k = 0;
+#pragma unroll
+  for (int b = 2; b >= 0; b--) k = (k << 3) | (((q[2] >> b) & 1u) << 2) | (((q[1] >> b) & 1u) << 1) | ((q[0] >> b) & 1u);
+  return k;
+}
+
+// Work decomposition.  A block owns one sink cell.  Its active sinks (up to
+// kPass per pass) are sorted by a 9-bit Morton key of their position in the
+// cell, then cut into groups of kGroup = 8 consecutive sinks (compact in
+// space).  Warps take groups round-robin.  For each group a warp streams the
+// staged neighbourhood, keeps the sources within rcut of the group's bounding
+// box (ballot + popc) and copies them contiguously into its float4 buffer;
+// lanes are (sink t = lane % 8) x (phase = lane / 8), so one step evaluates 8
+// sinks against 4 consecutive buffered sources (conflict-free broadcast-free
+// reads) and a fixed two-step shuffle reduction folds the 4 phases.  Per-sink
+// sums live in shared memory with Kahan compensation across chunks.
+//
+// Shared memory (dynamic): src[stage] float4 | buf[W][kBuf] float4 |
+// spos[kPass] float4 | acc[kPass][8] float | skey[kPass] | runb/runp.
+constexpr int kPass = 256;
+constexpr int kGroup = 8;
+constexpr int kBuf = 64;
+constexpr int kMaxRuns = 18;
+
+__global__ void __launch_bounds__(kKickThreads, 2) k_kick_pme(KickArgs a, int stage) {
+  extern __shared__ float4 smem4[];
+  const int T = blockDim.x, W = T >> 5;
+  float4* src = smem4;
+  float4* bufs = src + stage;
+  float4* spos = bufs + W * kBuf;
+  float* acc = reinterpret_cast<float*>(spos + kPass);
+  unsigned* skey = reinterpret_cast<unsigned*>(acc + kPass * 8);
+  int* runb = reinterpret_cast<int*>(skey + kPass);
+  int* runp = runb + kMaxRuns;
   const int C = a.C;
   int bid = blockIdx.x;
   const int i2 = bid % a.s2;
@@ -169,94 +217,196 @@ __global__ void __launch_bounds__(kKickThreads) k_kick_pme(KickArgs a) {
   const int64_t key = ((int64_t)cz * C + cy) * C + cx;
   const int32_t pb = __ldg(a.begin + key), pe = __ldg(a.begin + key + 1);
   if (pb == pe) return;
-  // sink cell centre in fixed point (offsets are taken from here)
   const uint32_t ox = (uint32_t)((((uint64_t)(2 * cx + 1)) << 31) / (uint64_t)C);
   const uint32_t oy = (uint32_t)((((uint64_t)(2 * cy + 1)) << 31) / (uint64_t)C);
   const uint32_t oz = (uint32_t)((((uint64_t)(2 * cz + 1)) << 31) / (uint64_t)C);
-  const int tid = threadIdx.x;
-  for (int32_t sbase = pb; sbase < pe; sbase += kKickThreads) {
-    const int32_t i = sbase + tid;
-    const bool active = i < pe && a.rung[i] >= a.min_rung;
-    float sx = 0.f, sy = 0.f, sz = 0.f;
-    float lx = 0.f, ly = 0.f, lz = 0.f, lp = 0.f;
-    if (active) {
-      const int4 q = __ldg(a.pos4 + i);
-      sx = distance32((uint32_t)q.x, ox);
-      sy = distance32((uint32_t)q.y, oy);
-      sz = distance32((uint32_t)q.z, oz);
-      interp_long(a, q, lx, ly, lz, lp);
-    }
-    float Sx = 0.f, Sy = 0.f, Sz = 0.f, Sp = 0.f;
-    float Cx = 0.f, Cy = 0.f, Cz = 0.f, Cp = 0.f;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int t8 = lane & 7, ph = lane >> 3;
+  const float Cf = (float)C;
+  const bool cull = a.rcut2 < INFINITY;
+  if (tid == 0) {
+    int nr = 0, tot = 0;
     for (int dz = -1; dz <= 1; dz++) {
       const int rz = wrapi(cz + dz, C);
       for (int dy = -1; dy <= 1; dy++) {
         const int ry = wrapi(cy + dy, C);
         const int64_t row = ((int64_t)rz * C + ry) * C;
-        int32_t rb[2], re[2];
-        int nrun;
+        int xa[2], xb[2], np;
         if (cx >= 1 && cx + 1 < C) {
-          rb[0] = __ldg(a.begin + row + cx - 1);
-          re[0] = __ldg(a.begin + row + cx + 2);
-          nrun = 1;
+          xa[0] = cx - 1; xb[0] = cx + 2; np = 1;
         } else if (cx == 0) {
-          rb[0] = __ldg(a.begin + row + C - 1);
-          re[0] = __ldg(a.begin + row + C);
-          rb[1] = __ldg(a.begin + row);
-          re[1] = __ldg(a.begin + row + 2);
-          nrun = 2;
+          xa[0] = C - 1; xb[0] = C; xa[1] = 0; xb[1] = 2; np = 2;
         } else {
-          rb[0] = __ldg(a.begin + row + C - 2);
-          re[0] = __ldg(a.begin + row + C);
-          rb[1] = __ldg(a.begin + row);
-          re[1] = __ldg(a.begin + row + 1);
-          nrun = 2;
+          xa[0] = C - 2; xb[0] = C; xa[1] = 0; xb[1] = 1; np = 2;
         }
-        for (int run = 0; run < nrun; run++) {
-          for (int32_t t0 = rb[run]; t0 < re[run]; t0 += kTile) {
-            const int len = min(kTile, re[run] - t0);
-            __syncthreads();
-            for (int j = tid; j < len; j += kKickThreads) {
-              const int4 q = __ldg(a.pos4 + t0 + j);
-              src[j] = make_float4(distance32((uint32_t)q.x, ox), distance32((uint32_t)q.y, oy),
-                                   distance32((uint32_t)q.z, oz), 0.f);
+        for (int p = 0; p < np; p++) {
+          const int32_t b = __ldg(a.begin + row + xa[p]), e = __ldg(a.begin + row + xb[p]);
+          runb[nr] = b;
+          runp[nr] = tot;
+          tot += e - b;
+          nr++;
+        }
+      }
+    }
+    for (int r = nr; r <= kMaxRuns; r++) runp[r] = tot;
+  }
+  __syncthreads();
+  const int total = runp[kMaxRuns];
+  float4* buf = bufs + warp * kBuf;
+  for (int32_t sbase = pb; sbase < pe; sbase += kPass) {
+    // 1. order this pass's active sinks by sub-cell (deterministic bitonic sort)
+    if (tid == 0) runp[kMaxRuns + 1] = kPass;  // active count when every slot is active
+    for (int e = tid; e < kPass; e += T) {
+      const int32_t i = sbase + e;
+      unsigned k = 512u;  // inactive / absent sinks sort last
+      if (i < pe && a.rung[i] >= a.min_rung) {
+        const int4 q = __ldg(a.pos4 + i);
+        k = morton9(distance32((uint32_t)q.x, ox), distance32((uint32_t)q.y, oy), distance32((uint32_t)q.z, oz), Cf);
+      }
+      skey[e] = (k << 8) | (unsigned)e;
+    }
+    __syncthreads();
+    for (int kk = 2; kk <= kPass; kk <<= 1) {
+      for (int j = kk >> 1; j > 0; j >>= 1) {
+        for (int e = tid; e < kPass; e += T) {
+          const int ixj = e ^ j;
+          if (ixj > e) {
+            const unsigned u = skey[e], v = skey[ixj];
+            const bool up = (e & kk) == 0;
+            if ((u > v) == up) {
+              skey[e] = v;
+              skey[ixj] = u;
             }
-            __syncthreads();
-            if (active) {
-              for (int jc = 0; jc < len; jc += kChunk) {
-                const int je = min(len, jc + kChunk);
-                float px = 0.f, py = 0.f, pz = 0.f, pp = 0.f;
-#pragma unroll 4
-                for (int j = jc; j < je; j++) {
-                  const float4 s = src[j];
-                  pair(a, sx - s.x, sy - s.y, sz - s.z, px, py, pz, pp);
-                }
-                if (a.kahan) {
-                  kahan_add(Sx, Cx, px);
-                  kahan_add(Sy, Cy, py);
-                  kahan_add(Sz, Cz, pz);
-                  kahan_add(Sp, Cp, pp);
-                } else {
-                  Sx += px;
-                  Sy += py;
-                  Sz += pz;
-                  Sp += pp;
-                }
-              }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int e = tid; e < kPass; e += T) {
+      const unsigned m = skey[e];
+      const bool act = (m >> 8) < 512u;
+      float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (act) {
+        const int4 q = __ldg(a.pos4 + sbase + (int32_t)(m & 0xffu));
+        p = make_float4(distance32((uint32_t)q.x, ox), distance32((uint32_t)q.y, oy), distance32((uint32_t)q.z, oz), 0.f);
+      }
+      spos[e] = p;
+#pragma unroll
+      for (int c = 0; c < 8; c++) acc[e * 8 + c] = 0.f;
+      // active sinks sort first: the first inactive slot is their count
+      if (!act && (e == 0 || (skey[e - 1] >> 8) < 512u)) runp[kMaxRuns + 1] = e;
+    }
+    __syncthreads();
+    const int nact = runp[kMaxRuns + 1];
+    const int ngroups = (nact + kGroup - 1) / kGroup;
+    for (int c0 = 0; c0 < total; c0 += stage) {
+      const int len = min(stage, total - c0);
+      __syncthreads();
+      for (int j = tid; j < len; j += T) {
+        const int e = c0 + j;
+        int r = 0;
+        while (runp[r + 1] <= e) r++;
+        const int4 u = __ldg(a.pos4 + runb[r] + (e - runp[r]));
+        src[j] = make_float4(distance32((uint32_t)u.x, ox), distance32((uint32_t)u.y, oy),
+                             distance32((uint32_t)u.z, oz), 0.f);
+      }
+      __syncthreads();
+      for (int g = warp; g < ngroups; g += W) {
+        const int gs = g * kGroup;
+        const int gn = min(kGroup, nact - gs);
+        const bool mysink = t8 < gn;
+        const float4 sp = spos[gs + (mysink ? t8 : 0)];
+        // group bounding box (lanes 0..gn-1 hold the sinks)
+        float bxl = mysink ? sp.x : INFINITY, bxh = mysink ? sp.x : -INFINITY;
+        float byl = mysink ? sp.y : INFINITY, byh = mysink ? sp.y : -INFINITY;
+        float bzl = mysink ? sp.z : INFINITY, bzh = mysink ? sp.z : -INFINITY;
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+          bxl = fminf(bxl, __shfl_xor_sync(0xffffffffu, bxl, o));
+          bxh = fmaxf(bxh, __shfl_xor_sync(0xffffffffu, bxh, o));
+          byl = fminf(byl, __shfl_xor_sync(0xffffffffu, byl, o));
+          byh = fmaxf(byh, __shfl_xor_sync(0xffffffffu, byh, o));
+          bzl = fminf(bzl, __shfl_xor_sync(0xffffffffu, bzl, o));
+          bzh = fmaxf(bzh, __shfl_xor_sync(0xffffffffu, bzh, o));
+        }
+        float px = 0.f, py = 0.f, pz = 0.f, pp = 0.f;
+        int cnt = 0;
+        for (int j0 = 0; j0 < len; j0 += 32) {
+          const int j = j0 + lane;
+          bool keep = j < len;
+          float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (keep) {
+            s = src[j];
+            if (cull) {
+              const float ex = fmaxf(fmaxf(bxl - s.x, s.x - bxh), 0.f);
+              const float ey = fmaxf(fmaxf(byl - s.y, s.y - byh), 0.f);
+              const float ez = fmaxf(fmaxf(bzl - s.z, s.z - bzh), 0.f);
+              keep = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.rcut2;
             }
+          }
+          const unsigned b = __ballot_sync(0xffffffffu, keep);
+          if (keep) buf[cnt + __popc(b & ((1u << lane) - 1u))] = s;
+          cnt += __popc(b);
+          __syncwarp();
+          if (cnt >= 32) {
+#pragma unroll
+            for (int k = 0; k < 32; k += 4) {
+              const float4 u = buf[k + ph];
+              if (mysink) pair(a, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
+            }
+            __syncwarp();
+            if (lane < cnt - 32) buf[lane] = buf[32 + lane];
+            cnt -= 32;
+            __syncwarp();
+          }
+        }
+        for (int k = 0; k < cnt; k += 4) {
+          if (k + ph < cnt && mysink) {
+            const float4 u = buf[k + ph];
+            pair(a, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
+          }
+        }
+        __syncwarp();
+        // fold the four source phases (fixed order), lanes 0..7 hold the group's sums
+#pragma unroll
+        for (int o = 8; o <= 16; o <<= 1) {
+          px += __shfl_xor_sync(0xffffffffu, px, o);
+          py += __shfl_xor_sync(0xffffffffu, py, o);
+          pz += __shfl_xor_sync(0xffffffffu, pz, o);
+          pp += __shfl_xor_sync(0xffffffffu, pp, o);
+        }
+        if (ph == 0 && mysink) {
+          float* A = acc + (gs + t8) * 8;
+          if (a.kahan) {
+            kahan_add(A[0], A[4], px);
+            kahan_add(A[1], A[5], py);
+            kahan_add(A[2], A[6], pz);
+            kahan_add(A[3], A[7], pp);
+          } else {
+            A[0] += px;
+            A[1] += py;
+            A[2] += pz;
+            A[3] += pp;
           }
         }
       }
     }
-    if (active) {
-      const float g0 = ((Sx - Cx) + lx) * a.GM;
-      const float g1 = ((Sy - Cy) + ly) * a.GM;
-      const float g2 = ((Sz - Cz) + lz) * a.GM;
-      const float ph = ((Sp - Cp) + lp) * a.GM;
+    __syncthreads();
+    // 2. long-range interpolation and the kick, one thread per sorted sink
+    for (int e = tid; e < nact; e += T) {
+      const int32_t i = sbase + (int32_t)(skey[e] & 0xffu);
+      const int4 q = __ldg(a.pos4 + i);
+      float lx, ly, lz, lp;
+      interp_long(a, q, lx, ly, lz, lp);
+      const float* A = acc + e * 8;
+      const float g0 = ((A[0] - A[4]) + lx) * a.GM;
+      const float g1 = ((A[1] - A[5]) + ly) * a.GM;
+      const float g2 = ((A[2] - A[6]) + lz) * a.GM;
+      const float phi = ((A[3] - A[7]) + lp) * a.GM;
       a.gx[i] = g0;
       a.gy[i] = g1;
       a.gz[i] = g2;
-      a.pot[i] = ph;
+      a.pot[i] = phi;
       // rung / velocity kick (src/kick_pme.cu:330-352); rung_dt[r] = 2^-r.
       int r = a.rung[i];
       if (r < 0 || r >= kMaxRung) {
@@ -284,6 +434,7 @@ __global__ void __launch_bounds__(kKickThreads) k_kick_pme(KickArgs a) {
       a.vy[i] = fmaf(g1, dt, vy);
       a.vz[i] = fmaf(g2, dt, vz);
     }
+    __syncthreads();  // sort keys / staging reused by the next pass
   }
 }
 
@@ -336,9 +487,20 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
   a.hinv = 1.f / a.hsoft;
   a.h3inv = a.hinv * (a.hinv * a.hinv);
   a.rcut2 = c->rcut_box > 0 ? (float)(c->rcut_box * c->rcut_box) : INFINITY;
+  // Block size follows the mean cell occupancy (about two groups of 8 sinks
+  // per warp, 2..8 warps); the stage holds 1.25x the mean 27-cell
+  // neighbourhood (at most kMaxStage sources; larger ones are chunked).
+  const double mean_cell = (double)c->n / ((double)C * C * C);
+  const int W = (int)std::min(8.0, std::max(2.0, std::ceil(mean_cell / (2.0 * kGroup))));
+  const int T = 32 * W;
+  int stage = (int)std::min<double>(kMaxStage, std::max<double>(512.0, 1.25 * 27.0 * mean_cell));
+  stage = (stage + 127) / 128 * 128;
+  const size_t smem = sizeof(float4) * ((size_t)stage + (size_t)W * kBuf + kPass) + sizeof(float) * kPass * 8 +
+                      sizeof(unsigned) * kPass + sizeof(int) * (2 * kMaxRuns + 2);
+  TPM_CUDA_TRY(cudaFuncSetAttribute(k_kick_pme, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   stage_begin(c, kStKick);
   if (ncell > 0) {
-    k_kick_pme<<<(unsigned)ncell, kKickThreads, 0, c->stream>>>(a);
+    k_kick_pme<<<(unsigned)ncell, T, smem, c->stream>>>(a, stage);
     c->launches++;
     TPM_CUDA_TRY(cudaGetLastError());
   }

@@ -20,11 +20,11 @@ int fail(int status, const std::string& msg) {
 }
 
 void stage_begin(tpm_ctx* c, Stage s) {
-  cudaEventRecord(c->ev.beg[s], c->stream);
+  cudaEventRecord(c->ev.beg[s][c->ev.count[s] % kStageSlots], c->stream);
 }
 void stage_end(tpm_ctx* c, Stage s) {
-  cudaEventRecord(c->ev.end[s], c->stream);
-  c->ev.used[s] = true;
+  cudaEventRecord(c->ev.end[s][c->ev.count[s] % kStageSlots], c->stream);
+  c->ev.count[s]++;
 }
 
 }  // namespace tpm
@@ -244,9 +244,11 @@ int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out) {
     return fail(TPM_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
   }
   for (int s = 0; s < 8; s++) {
-    cudaEventCreate(&c->ev.beg[s]);
-    cudaEventCreate(&c->ev.end[s]);
-    c->ev.used[s] = false;
+    for (int k = 0; k < kStageSlots; k++) {
+      cudaEventCreate(&c->ev.beg[s][k]);
+      cudaEventCreate(&c->ev.end[s][k]);
+    }
+    c->ev.count[s] = 0;
   }
   c->cap = capacity;
   const int64_t N = c->N, C = c->C, ncell = C * C * C;
@@ -322,8 +324,10 @@ int tpm_ctx_destroy(tpm_ctx* c) {
     cufftDestroy(c->plan_c2r);
   }
   for (int s = 0; s < 8; s++) {
-    if (c->ev.beg[s]) cudaEventDestroy(c->ev.beg[s]);
-    if (c->ev.end[s]) cudaEventDestroy(c->ev.end[s]);
+    for (int k = 0; k < kStageSlots; k++) {
+      if (c->ev.beg[s][k]) cudaEventDestroy(c->ev.beg[s][k]);
+      if (c->ev.end[s][k]) cudaEventDestroy(c->ev.end[s][k]);
+    }
   }
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -582,9 +586,17 @@ int tpm_get_stage_times(tpm_ctx* c, tpm_stage_times* out) {
   TPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
   float t[8] = {0};
   for (int s = 0; s < 8; s++) {
-    if (c->ev.used[s]) {
-      if (cudaEventElapsedTime(&t[s], c->ev.beg[s], c->ev.end[s]) != cudaSuccess) t[s] = -1.f;
+    const int64_t n = std::min<int64_t>(c->ev.count[s], kStageSlots);
+    double sum = 0;
+    for (int64_t k = 0; k < n; k++) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, c->ev.beg[s][k], c->ev.end[s][k]) != cudaSuccess) {
+        sum = -1;
+        break;
+      }
+      sum += ms;
     }
+    t[s] = n > 0 && sum >= 0 ? (float)(sum / n) : (n > 0 ? -1.f : 0.f);
   }
   out->sort_ms = t[kStSort];
   out->deposit_ms = t[kStDeposit];
@@ -594,6 +606,13 @@ int tpm_get_stage_times(tpm_ctx* c, tpm_stage_times* out) {
   out->kick_ms = t[kStKick];
   out->drift_ms = t[kStDrift];
   out->ewald_ms = t[kStEwald];
+  return TPM_OK;
+}
+
+int tpm_reset_stage_times(tpm_ctx* c) {
+  if (!c) return fail(TPM_ERR_INVALID, "null argument");
+  TPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (int s = 0; s < 8; s++) c->ev.count[s] = 0;
   return TPM_OK;
 }
 

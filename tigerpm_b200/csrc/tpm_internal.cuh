@@ -43,10 +43,13 @@ struct TreeNode {
   int lo, mid, hi, pad;
 };
 
+// Per-stage CUDA event pairs, a ring of kStageSlots launches per stage, so
+// that the average over many steps can be read after they ran.
+constexpr int kStageSlots = 64;
 struct StageEvents {
-  cudaEvent_t beg[8];
-  cudaEvent_t end[8];
-  bool used[8];
+  cudaEvent_t beg[8][kStageSlots];
+  cudaEvent_t end[8][kStageSlots];
+  int64_t count[8];   // records since the last reset
 };
 
 enum Stage { kStSort = 0, kStDeposit, kStFftF, kStGreen, kStFftI, kStKick, kStDrift, kStEwald };
