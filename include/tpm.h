@@ -92,6 +92,8 @@ typedef struct tpm_options {
   int deconv_order;    /* sinc^-p deconvolution; 0: assignment order (4/2/3) */
   int sort_mode;       /* TPM_SORT_*; default PARITY */
   int kahan;           /* 1: compensated per-target PP sums (default 1) */
+  int deterministic_deposit; /* 1: exact int64 fixed-point deposit, bit-reproducible;
+                              * 0: FP32 shared-memory atomics (default, faster) */
   uint64_t seed;       /* synthetic-input seed carried for drivers */
 } tpm_options;
 

@@ -41,7 +41,8 @@ class Options(C.Structure):
         ("box_size", C.c_double), ("rs", C.c_double), ("omega_m", C.c_double),
         ("z0", C.c_double),
         ("rcut_over_rs", C.c_double), ("assign", C.c_int), ("deconv_order", C.c_int),
-        ("sort_mode", C.c_int), ("kahan", C.c_int), ("seed", C.c_uint64),
+        ("sort_mode", C.c_int), ("kahan", C.c_int), ("deterministic_deposit", C.c_int),
+        ("seed", C.c_uint64),
     ]
 
 

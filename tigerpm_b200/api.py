@@ -75,7 +75,7 @@ def process_options(argv) -> Options:
 
 def make_options(n_side: int, grid: int, chain: int | None = None, rs_cells: float = 1.0,
                  rcut_over_rs: float = 0.0, assign: str = "cloud4", sort: str = "parity",
-                 kahan: bool = True, GM: float = 1.0) -> Options:
+                 kahan: bool = True, GM: float = 1.0, deterministic_deposit: bool = False) -> Options:
     """Options for a box of n_side^3 particles on a grid^3 mesh.  chain=None
     picks the largest chain mesh whose cells are at least the cutoff wide
     (or rcut = 4.5 rs wide when there is no cutoff)."""
@@ -91,6 +91,7 @@ def make_options(n_side: int, grid: int, chain: int | None = None, rs_cells: flo
     o.assign = _lib.ASSIGN[assign]
     o.sort_mode = _lib.SORT[sort]
     o.kahan = 1 if kahan else 0
+    o.deterministic_deposit = 1 if deterministic_deposit else 0
     o.GM = GM
     return o
 

@@ -186,126 +186,200 @@ struct LevelArgs {
   const int* __restrict__ depth;
 };
 
-// The recursion node that owns position p at this depth: its position range
-// [b, e), the split point pm (first position of the right child), the split
-// dim's mid cell and the particle's coordinate along that dim.  Returns false
-// when the cell holding p is already a leaf at this depth.
-__device__ __forceinline__ bool node_of(const LevelArgs& a, int64_t p, int32_t& b, int32_t& pm,
-                                        int32_t& e, bool& is_left_flag) {
-  const int cell = a.cellof[p];
+// The recursion node that owns positions of final cell `cell` at this depth:
+// its position range [b, e), the split point pm (first position of the right
+// child), the split dim (0..2) and mid cell.  Returns false when the cell is
+// already a leaf at this depth.
+struct Node {
+  int32_t b, pm, e;
+  int dim, mid;
+  bool live;
+};
+
+__device__ __forceinline__ Node node_of_cell(const LevelArgs& a, int cell) {
+  Node nd;
   const int C = a.C;
   const int cx = cell % C, cy = (cell / C) % C, cz = cell / (C * C);
   const int dz = __ldg(a.depth + cz), dy = __ldg(a.depth + cy), dx = __ldg(a.depth + cx);
-  const uint32_t k = a.key[p];
-  const int kx = (int)(k % (uint32_t)C), ky = (int)((k / (uint32_t)C) % (uint32_t)C),
-            kz = (int)(k / ((uint32_t)C * (uint32_t)C));
   int l = a.level;
   const int64_t CC = (int64_t)C * C;
+  nd.live = true;
   if (l < dz) {
     const TreeNode t = a.tree[cz * kMaxTreeDepth + l];
-    b = __ldg(a.begin + t.lo * CC);
-    pm = __ldg(a.begin + t.mid * CC);
-    e = __ldg(a.begin + t.hi * CC);
-    is_left_flag = kz < t.mid;
-    return true;
+    nd.b = __ldg(a.begin + t.lo * CC);
+    nd.pm = __ldg(a.begin + t.mid * CC);
+    nd.e = __ldg(a.begin + t.hi * CC);
+    nd.dim = 2;
+    nd.mid = t.mid;
+    return nd;
   }
   l -= dz;
   if (l < dy) {
     const TreeNode t = a.tree[cy * kMaxTreeDepth + l];
     const int64_t base = (int64_t)cz * C;
-    b = __ldg(a.begin + (base + t.lo) * C);
-    pm = __ldg(a.begin + (base + t.mid) * C);
-    e = __ldg(a.begin + (base + t.hi) * C);
-    is_left_flag = ky < t.mid;
-    return true;
+    nd.b = __ldg(a.begin + (base + t.lo) * C);
+    nd.pm = __ldg(a.begin + (base + t.mid) * C);
+    nd.e = __ldg(a.begin + (base + t.hi) * C);
+    nd.dim = 1;
+    nd.mid = t.mid;
+    return nd;
   }
   l -= dy;
   if (l < dx) {
     const TreeNode t = a.tree[cx * kMaxTreeDepth + l];
     const int64_t base = ((int64_t)cz * C + cy) * C;
-    b = __ldg(a.begin + base + t.lo);
-    pm = __ldg(a.begin + base + t.mid);
-    e = __ldg(a.begin + base + t.hi);
-    is_left_flag = kx < t.mid;
-    return true;
+    nd.b = __ldg(a.begin + base + t.lo);
+    nd.pm = __ldg(a.begin + base + t.mid);
+    nd.e = __ldg(a.begin + base + t.hi);
+    nd.dim = 0;
+    nd.mid = t.mid;
+    return nd;
   }
-  return false;
+  nd.live = false;
+  nd.b = nd.pm = nd.e = 0;
+  nd.dim = 0;
+  nd.mid = 0;
+  return nd;
 }
 
-// f(p) = 1 when the particle at p belongs to the LEFT child (x < xmid).
-__device__ __forceinline__ int level_flag(const LevelArgs& a, int64_t p) {
-  int32_t b, pm, e;
-  bool left;
-  if (p >= a.n || !node_of(a, p, b, pm, e, left)) return 0;
-  return left ? 1 : 0;
+// f = 1 when the particle with cell key k belongs to the node's LEFT child
+// (its coordinate along the split dim is below mid, i.e. x < xmid).
+__device__ __forceinline__ int left_flag(const Node& nd, uint32_t k, int C) {
+  if (!nd.live) return 0;
+  const uint32_t uc = (uint32_t)C;
+  const int c = nd.dim == 0 ? (int)(k % uc) : nd.dim == 1 ? (int)((k / uc) % uc) : (int)(k / (uc * uc));
+  return c < nd.mid ? 1 : 0;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_level_blocksum(LevelArgs a, int32_t* __restrict__ bsum) {
+// Node lookups are cached while consecutive positions share a final cell
+// (cells hold many particles), which removes most dependent loads.
+struct NodeCache {
+  int cell = -1;
+  Node nd;
+  __device__ __forceinline__ const Node& get(const LevelArgs& a, int c) {
+    if (c != cell) {
+      cell = c;
+      nd = node_of_cell(a, c);
+    }
+    return nd;
+  }
+};
+
+// Decoupled look-back scan status word: stamp (30 bits) | flag (2 bits) | value (32 bits).
+constexpr unsigned long long kFlagAgg = 1ull, kFlagIncl = 2ull;
+__device__ __forceinline__ unsigned long long pack_status(unsigned stamp, unsigned long long flag, int value) {
+  return ((unsigned long long)stamp << 34) | (flag << 32) | (unsigned long long)(unsigned)value;
+}
+
+// One partition level, part 1: the left-child flags of every position and
+// their exclusive prefix, in a single pass (chained scan with decoupled
+// look-back; tiles are taken in launch order through an atomic counter, so
+// every predecessor a tile waits on is already running).  The look-back spin
+// is bounded: on expiry the tile records kErrTimeout and uses 0.
+__global__ void __launch_bounds__(kScanThreads) k_level_scan(LevelArgs a, unsigned stamp, int* __restrict__ counter,
+                                                             unsigned long long* __restrict__ status,
+                                                             int32_t* __restrict__ prefix, int* __restrict__ err) {
   __shared__ int warp_tot[32];
   __shared__ int total;
-  const int64_t base = (int64_t)blockIdx.x * kScanTile;
-  int s = 0;
-#pragma unroll
-  for (int k = 0; k < kScanItems; k++) s += level_flag(a, base + (int64_t)threadIdx.x * kScanItems + k);
-  block_exclusive_scan(s, warp_tot, &total);
-  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
-}
-
-__global__ void __launch_bounds__(kScanThreads) k_level_prefix(LevelArgs a, const int32_t* __restrict__ boff,
-                                                               int32_t* __restrict__ prefix) {
-  __shared__ int warp_tot[32];
-  __shared__ int total;
-  const int64_t base = (int64_t)blockIdx.x * kScanTile;
+  __shared__ int tile_s;
+  __shared__ int excl_s;
+  if (threadIdx.x == 0) tile_s = atomicAdd(counter, 1);
+  __syncthreads();
+  const int tile = tile_s;
+  const int64_t base = (int64_t)tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
   int v[kScanItems];
   int s = 0;
+  NodeCache cache;
 #pragma unroll
   for (int k = 0; k < kScanItems; k++) {
-    v[k] = level_flag(a, base + (int64_t)threadIdx.x * kScanItems + k);
+    const int64_t p = base + k;
+    v[k] = 0;
+    if (p < a.n) v[k] = left_flag(cache.get(a, a.cellof[p]), a.key[p], a.C);
     s += v[k];
   }
-  int off = block_exclusive_scan(s, warp_tot, &total) + boff[blockIdx.x];
+  const int off = block_exclusive_scan(s, warp_tot, &total);
+  if (threadIdx.x == 0) {
+    const int agg = total;
+    int excl = 0;
+    if (tile == 0) {
+      atomicExch(status, pack_status(stamp, kFlagIncl, agg));
+    } else {
+      atomicExch(status + tile, pack_status(stamp, kFlagAgg, agg));
+      int j = tile - 1;
+      long long spins = 0;
+      while (j >= 0) {
+        const unsigned long long w = *reinterpret_cast<volatile unsigned long long*>(status + j);
+        const unsigned wstamp = (unsigned)(w >> 34);
+        const unsigned long long f = (w >> 32) & 3ull;
+        if (wstamp != stamp || f == 0) {
+          if (++spins > (1ll << 24)) {
+            atomicOr(err, kErrTimeout);
+            break;
+          }
+          continue;
+        }
+        excl += (int)(unsigned)(w & 0xffffffffull);
+        if (f == kFlagIncl) break;
+        j--;
+      }
+      atomicExch(status + tile, pack_status(stamp, kFlagIncl, excl + agg));
+    }
+    excl_s = excl;
+  }
+  __syncthreads();
+  int run = excl_s + off;
 #pragma unroll
   for (int k = 0; k < kScanItems; k++) {
-    const int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
-    if (i < a.n) prefix[i] = off;
-    off += v[k];
+    const int64_t p = base + k;
+    if (p < a.n) prefix[p] = run;
+    run += v[k];
   }
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) prefix[a.n] = boff[gridDim.x];
+  if (base < a.n && base + kScanItems >= a.n) prefix[a.n] = run;  // the thread holding position n-1
 }
 
-// Right-part elements that belong left (x < xmid) are the two-pointer's
-// swap partners, met in descending order: the k-th from the end of the node
-// goes to slot[b + k].
-__global__ void k_level_slots(LevelArgs a, const int32_t* __restrict__ prefix, int32_t* __restrict__ slot) {
-  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (p >= a.n) return;
-  int32_t b, pm, e;
-  bool left;
-  if (!node_of(a, p, b, pm, e, left)) return;
-  if (p >= pm && left) {
-    const int32_t k = prefix[e] - prefix[p] - 1;  // flagged elements in (p, e)
-    slot[b + k] = (int32_t)p;
+// Part 2: right-part elements that belong left (x < xmid) are the
+// two-pointer's swap partners, met in descending order: the k-th from the
+// end of the node goes to slot[b + k].
+__global__ void __launch_bounds__(256) k_level_slots(LevelArgs a, const int32_t* __restrict__ prefix,
+                                                     int32_t* __restrict__ slot) {
+  const int64_t p0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 4;
+  NodeCache cache;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int64_t p = p0 + k;
+    if (p >= a.n) return;
+    const Node& nd = cache.get(a, a.cellof[p]);
+    if (!nd.live || p < nd.pm) continue;
+    if (left_flag(nd, a.key[p], a.C)) {
+      const int32_t kk = prefix[nd.e] - prefix[p] - 1;  // flagged elements in (p, e)
+      slot[nd.b + kk] = (int32_t)p;
+    }
   }
 }
 
-// Left-part elements that belong right swap with their partner: the k-th
-// such element from the start of the node pairs with slot[b + k].
-__global__ void k_level_swap(LevelArgs a, const int32_t* __restrict__ prefix, const int32_t* __restrict__ slot,
-                             uint32_t* __restrict__ key, int32_t* __restrict__ idx) {
-  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (p >= a.n) return;
-  int32_t b, pm, e;
-  bool left;
-  if (!node_of(a, p, b, pm, e, left)) return;
-  if (p < pm && !left) {
-    const int32_t k = (int32_t)(p - b) - (prefix[p] - prefix[b]);  // unflagged in [b, p)
-    const int32_t q = slot[b + k];
-    const uint32_t kp = key[p], kq = key[q];
-    const int32_t ip = idx[p], iq = idx[q];
-    key[p] = kq;
-    key[q] = kp;
-    idx[p] = iq;
-    idx[q] = ip;
+// Part 3: left-part elements that belong right swap with their partner: the
+// k-th such element from the start of the node pairs with slot[b + k].
+__global__ void __launch_bounds__(256) k_level_swap(LevelArgs a, const int32_t* __restrict__ prefix,
+                                                    const int32_t* __restrict__ slot, uint32_t* __restrict__ key,
+                                                    int32_t* __restrict__ idx) {
+  const int64_t p0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 4;
+  NodeCache cache;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int64_t p = p0 + k;
+    if (p >= a.n) return;
+    const Node& nd = cache.get(a, a.cellof[p]);
+    if (!nd.live || p >= nd.pm) continue;
+    if (!left_flag(nd, key[p], a.C)) {
+      const int32_t kk = (int32_t)(p - nd.b) - (prefix[p] - prefix[nd.b]);  // unflagged in [b, p)
+      const int32_t q = slot[nd.b + kk];
+      const uint32_t kp = key[p], kq = key[q];
+      const int32_t ip = idx[p], iq = idx[q];
+      key[p] = kq;
+      key[q] = kp;
+      idx[p] = iq;
+      idx[q] = ip;
+    }
   }
 }
 
@@ -439,14 +513,18 @@ int chainmesh_sort(tpm_ctx* c) {
       c->launches++;
       const int nb = ceil_div(n, kScanTile);
       const int levels = 3 * c->max_depth1d;
+      // per-level tile counters (zeroed once) and look-back status words
+      int* counters = c->cell_count;  // reused: C^3 + 1 >= levels ints after the scan above
+      unsigned long long* status = c->scan_status;
+      TPM_CUDA_TRY(cudaMemsetAsync(counters, 0, sizeof(int) * (levels + 1), s));
+      const int nq = ceil_div(n, 4);
       for (int l = 0; l < levels; l++) {
         LevelArgs a{n, C, l, c->cellof, c->key, c->cell_begin, c->tree, c->depth1d};
-        k_level_blocksum<<<nb, kScanThreads, 0, s>>>(a, c->blocksum);
-        k_scan_single<<<1, kScanThreads, 0, s>>>(c->blocksum, nb, c->blocksum + nb + 1);
-        k_level_prefix<<<nb, kScanThreads, 0, s>>>(a, c->blocksum + nb + 1, c->prefix);
-        k_level_slots<<<ceil_div(n, 256), 256, 0, s>>>(a, c->prefix, c->slot);
-        k_level_swap<<<ceil_div(n, 256), 256, 0, s>>>(a, c->prefix, c->slot, c->key, c->idx);
-        c->launches += 5;
+        const unsigned stamp = (unsigned)(++c->scan_stamp & 0x3fffffff);
+        k_level_scan<<<nb, kScanThreads, 0, s>>>(a, stamp, counters + l, status, c->prefix, c->d_err);
+        k_level_slots<<<ceil_div(nq, 256), 256, 0, s>>>(a, c->prefix, c->slot);
+        k_level_swap<<<ceil_div(nq, 256), 256, 0, s>>>(a, c->prefix, c->slot, c->key, c->idx);
+        c->launches += 3;
       }
     }
     k_gather<<<ceil_div(n, 256), 256, 0, s>>>(n, c->idx, c->x, c->y, c->z, c->vx, c->vy, c->vz, c->rung,

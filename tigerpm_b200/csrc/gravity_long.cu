@@ -11,10 +11,11 @@
 //  * deposit: "owner computes" mesh tiles.  One block owns a T^3 tile of the
 //    grid, reads the particles of the chain cells whose assignment stencils
 //    can reach it (particles are already in chain-cell order), and
-//    accumulates the weights in shared memory as 40-bit fixed-point int64.
-//    Integer addition is associative, so the grid is bit-for-bit
-//    reproducible whatever the thread order; each grid point is written once,
-//    with no global atomics and no zeroing pass.
+//    accumulates the weights in shared memory; each grid point is written
+//    once, with no global atomics and no zeroing pass.  Accumulation is FP32
+//    shared atomics by default, or (deterministic_deposit) exact 40-bit
+//    fixed point in int64, whose integer sums are bit-for-bit reproducible
+//    whatever the thread order.
 //  * FFT: cuFFT r2c / c2r (the library the project allows here), timed as
 //    its own stages.
 //  * Green's function: exp(-k^2 rs^2) * sinc(k/2)^-p factorises per axis, so
@@ -75,10 +76,32 @@ struct DepositArgs {
   float* __restrict__ rho;
 };
 
-template <int T, int ASSIGN>
+// Accumulator of one tile point: exact 40-bit fixed point in int64 (order
+// independent, bit-reproducible) or FP32 shared atomics (faster, rounding
+// depends on the order in which threads reach a point).
+template <bool EXACT>
+struct DepAcc;
+template <>
+struct DepAcc<true> {
+  using T = unsigned long long;
+  static __device__ __forceinline__ void add(T* p, float w) {
+    atomicAdd(p, (unsigned long long)__float2ll_rn(w * 1099511627776.0f));
+  }
+  static __device__ __forceinline__ double value(T v, double scale) { return (double)(long long)v * scale; }
+};
+template <>
+struct DepAcc<false> {
+  using T = float;
+  static __device__ __forceinline__ void add(T* p, float w) { atomicAdd(p, w); }
+  static __device__ __forceinline__ double value(T v, double scale) { return (double)v * scale; }
+};
+
+template <int T, int ASSIGN, bool EXACT>
 __global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
   constexpr int W = Width<ASSIGN>::W;
-  __shared__ unsigned long long acc[T * T * T];
+  using A = DepAcc<EXACT>;
+  extern __shared__ __align__(16) unsigned char dep_smem[];
+  typename A::T* acc = reinterpret_cast<typename A::T*>(dep_smem);
   const int N = a.N, C = a.C;
   int tb = blockIdx.x;
   const int tz = tb % a.ntile;
@@ -88,7 +111,7 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
   const int o[3] = {tx * T, ty * T, tz * T};
   int ext[3];
   for (int d = 0; d < 3; d++) ext[d] = min(T, N - o[d]);
-  for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) acc[i] = 0ull;
+  for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) acc[i] = 0;
   // chain cells whose particles can reach the tile: XN in [o-2, o+T+1)
   int clo[3], cnt[3];
   for (int d = 0; d < 3; d++) {
@@ -99,8 +122,6 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
     if (cnt[d] == C) clo[d] = 0;
   }
   __syncthreads();
-  const unsigned long long one = 1ull << kDepositFracBits;
-  const float fone = (float)one;
   for (int iz = 0; iz < cnt[2]; iz++) {
     const int cz = wrapi(clo[2] + iz, C);
     for (int iy = 0; iy < cnt[1]; iy++) {
@@ -149,11 +170,11 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
             for (int j = 0; j < W; j++) {
               if (li[1][j] < 0) continue;
               const float wxy = wx[i] * wy[j];
+              typename A::T* row_acc = acc + (li[0][i] * T + li[1][j]) * T;
 #pragma unroll
               for (int k = 0; k < W; k++) {
                 if (li[2][k] < 0) continue;
-                const long long v = __float2ll_rn(wxy * wz[k] * fone);
-                atomicAdd(&acc[(li[0][i] * T + li[1][j]) * T + li[2][k]], (unsigned long long)v);
+                A::add(row_acc + li[2][k], wxy * wz[k]);
               }
             }
           }
@@ -164,10 +185,8 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
   __syncthreads();
   for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) {
     const int lz = i % T, ly = (i / T) % T, lx = i / (T * T);
-    if (lx < ext[0] && ly < ext[1] && lz < ext[2]) {
-      const double v = (double)(long long)acc[i] * a.scale;
-      a.rho[((int64_t)(o[0] + lx) * N + (o[1] + ly)) * N + (o[2] + lz)] = (float)v;
-    }
+    if (lx < ext[0] && ly < ext[1] && lz < ext[2])
+      a.rho[((int64_t)(o[0] + lx) * N + (o[1] + ly)) * N + (o[2] + lz)] = (float)A::value(acc[i], a.scale);
   }
 }
 
@@ -241,19 +260,32 @@ __global__ void k_force_at(const float* __restrict__ phi, int N, int64_t n, cons
   for (int d = 0; d < 3; d++) g_out[3 * p + d] = (float)(-g[d]);
 }
 
-template <int T>
-void launch_deposit_T(tpm_ctx* c, const DepositArgs& a, int blocks) {
+template <int T, bool EXACT>
+int launch_deposit_T(tpm_ctx* c, DepositArgs a) {
+  a.ntile = ceil_div(c->N, T);
+  const int blocks = a.ntile * a.ntile * a.ntile;
+  const size_t smem = sizeof(typename DepAcc<EXACT>::T) * T * T * T;
+  a.scale = 4.0 * M_PI * c->N * (EXACT ? std::ldexp(1.0, -kDepositFracBits) : 1.0);
   switch (c->opt.assign) {
     case TPM_ASSIGN_CIC:
-      k_deposit<T, TPM_ASSIGN_CIC><<<blocks, 256, 0, c->stream>>>(a);
+      TPM_CUDA_TRY(cudaFuncSetAttribute(k_deposit<T, TPM_ASSIGN_CIC, EXACT>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_deposit<T, TPM_ASSIGN_CIC, EXACT><<<blocks, 256, smem, c->stream>>>(a);
       break;
     case TPM_ASSIGN_TSC:
-      k_deposit<T, TPM_ASSIGN_TSC><<<blocks, 256, 0, c->stream>>>(a);
+      TPM_CUDA_TRY(cudaFuncSetAttribute(k_deposit<T, TPM_ASSIGN_TSC, EXACT>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_deposit<T, TPM_ASSIGN_TSC, EXACT><<<blocks, 256, smem, c->stream>>>(a);
       break;
     default:
-      k_deposit<T, TPM_ASSIGN_CLOUD4><<<blocks, 256, 0, c->stream>>>(a);
+      TPM_CUDA_TRY(cudaFuncSetAttribute(k_deposit<T, TPM_ASSIGN_CLOUD4, EXACT>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_deposit<T, TPM_ASSIGN_CLOUD4, EXACT><<<blocks, 256, smem, c->stream>>>(a);
       break;
   }
+  c->launches++;
+  TPM_CUDA_TRY(cudaGetLastError());
+  return TPM_OK;
 }
 
 }  // namespace
@@ -284,7 +316,6 @@ int mesh_init(tpm_ctx* c) {
   TPM_CUFFT_TRY(cufftSetStream(c->plan_r2c, c->stream));
   TPM_CUFFT_TRY(cufftSetStream(c->plan_c2r, c->stream));
   c->plans = true;
-  c->deposit_tile = N >= 256 ? 16 : 8;
   (void)Nh;
   return TPM_OK;
 }
@@ -300,17 +331,19 @@ int gravity_long(tpm_ctx* c, int type) {
   a.begin = c->cell_begin;
   a.C = c->C;
   a.N = N;
-  a.scale = 4.0 * M_PI * N * std::ldexp(1.0, -kDepositFracBits);
+  a.ntile = 0;
+  a.scale = 0;
   a.rho = c->rho;
-  if (c->deposit_tile == 16) {
-    a.ntile = ceil_div(N, 16);
-    launch_deposit_T<16>(c, a, a.ntile * a.ntile * a.ntile);
+  int rc;
+  // tile edge: 24 points on large meshes (fewer redundant particle visits),
+  // 16 / 8 on smaller ones; exact (int64) tiles of 24^3 would need 110 KB.
+  if (c->opt.deterministic_deposit) {
+    rc = N >= 128 ? launch_deposit_T<16, true>(c, a) : launch_deposit_T<8, true>(c, a);
   } else {
-    a.ntile = ceil_div(N, 8);
-    launch_deposit_T<8>(c, a, a.ntile * a.ntile * a.ntile);
+    rc = N >= 192 ? launch_deposit_T<24, false>(c, a) : (N >= 64 ? launch_deposit_T<16, false>(c, a)
+                                                                  : launch_deposit_T<8, false>(c, a));
   }
-  c->launches++;
-  TPM_CUDA_TRY(cudaGetLastError());
+  if (rc) return rc;
   stage_end(c, kStDeposit);
   stage_begin(c, kStFftF);
   TPM_CUFFT_TRY(cufftExecR2C(c->plan_r2c, c->rho, c->rhok));

@@ -111,6 +111,7 @@ int tpm_check_errors(tpm_ctx* c) {
   if (err) {
     TPM_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
     TPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (err & kErrTimeout) return fail(TPM_ERR_TIMEOUT, "a bounded device wait (scan look-back) gave up");
     if (err & kErrRung) return fail(TPM_ERR_RUNG, "a new rung fell outside [0, 32) and was clamped");
     return fail(TPM_ERR_INVALID, "a drift step exceeded 2^31 box lengths");
   }

@@ -60,6 +60,7 @@ int64_t plan_bytes(const tpm_options& o, int64_t cap) {
   b += cap * 16;                               // pos4
   b += cap * 4 * 5 + 8;                        // key, idx, cellof, prefix, slot
   b += 4 * (2 * ((cap + 4095) / 4096 + (ncell + 4095) / 4096) + 64);  // blocksums
+  b += 8 * ((std::max(cap, ncell) + 4095) / 4096 + 1);  // look-back status words
   b += 8 * (ncell + 2);                        // counts + offsets
   b += N * N * N * 4 * 2 + N * N * (N / 2 + 1) * 8;  // rho, phi, rhok
   return b;
@@ -149,6 +150,7 @@ int tpm_options_init(tpm_options* o, int parts_dim, int parts_o_four, int four_o
   o->deconv_order = 0;
   o->sort_mode = TPM_SORT_PARITY;
   o->kahan = 1;
+  o->deterministic_deposit = 0;
   o->seed = 1;
   return TPM_OK;
 }
@@ -156,7 +158,7 @@ int tpm_options_init(tpm_options* o, int parts_dim, int parts_o_four, int four_o
 int tpm_options_parse(tpm_options* o, int argc, const char* const* argv) {
   if (!o) return fail(TPM_ERR_INVALID, "null options");
   int parts_dim = 130, parts_o_four = 3, four_o_chain = 5;  // src/options.cpp:50-52 defaults
-  int four_dim = 0, chain_dim = 0, kahan = 1, sort_mode = 0, assign = 0;
+  int four_dim = 0, chain_dim = 0, kahan = 1, sort_mode = 0, assign = 0, det_dep = 0;
   double rs_cells = 0, rcut = 0, hsoft = 0, box_size = 1;
   unsigned long long seed = 1;
   for (int i = 0; i < argc; i++) {
@@ -180,6 +182,7 @@ int tpm_options_parse(tpm_options* o, int argc, const char* const* argv) {
     else if (key == "rcut_over_rs") ok = parse_double(val.c_str(), &rcut);
     else if (key == "hsoft") ok = parse_double(val.c_str(), &hsoft);
     else if (key == "kahan") ok = parse_int(val.c_str(), &kahan);
+    else if (key == "deterministic_deposit") ok = parse_int(val.c_str(), &det_dep);
     else if (key == "seed") seed = strtoull(val.c_str(), nullptr, 10);
     else if (key == "assign") {
       if (val == "cloud4") assign = 0;
@@ -216,6 +219,7 @@ int tpm_options_parse(tpm_options* o, int argc, const char* const* argv) {
   o->assign = assign;
   o->sort_mode = sort_mode;
   o->kahan = kahan;
+  o->deterministic_deposit = det_dep;
   o->seed = seed;
   return TPM_OK;
 }
@@ -279,6 +283,7 @@ int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out) {
   A.get(c->prefix, capacity + 1);
   A.get(c->slot, capacity);
   A.get(c->blocksum, 2 * nb + 64);
+  A.get(c->scan_status, nb + 1);
   A.get(c->cell_count, ncell + 1);
   A.get(c->cell_begin, ncell + 1);
   A.get(c->thr, C + 1);
@@ -295,6 +300,7 @@ int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out) {
     return A.status;
   }
   e = cudaMemset(c->d_err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->scan_status, 0, sizeof(unsigned long long) * (nb + 1));
   if (e == cudaSuccess) e = cudaMemset(c->cell_begin, 0, sizeof(int32_t) * (ncell + 1));
   if (e != cudaSuccess) {
     tpm_ctx_destroy(c);
@@ -315,7 +321,7 @@ int tpm_ctx_destroy(tpm_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->x, c->y, c->z, c->vx, c->vy, c->vz, c->rung, c->gx, c->gy, c->gz, c->pot, c->pos4,
                   c->x2, c->y2, c->z2, c->vx2, c->vy2, c->vz2, c->rung2, c->key, c->idx, c->cellof,
-                  c->prefix, c->slot, c->blocksum, c->cell_count, c->cell_begin, c->thr, c->tree,
+                  c->prefix, c->slot, c->blocksum, c->scan_status, c->cell_count, c->cell_begin, c->thr, c->tree,
                   c->depth1d, c->rho, c->rhok, c->phi, c->gtab, c->k2tab, c->d_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);

@@ -21,6 +21,7 @@ constexpr int kDepositFracBits = 40;
 // Error bits a kernel may raise in ctx->d_err (never a trap).
 constexpr int kErrRung = 1;
 constexpr int kErrBounds = 2;
+constexpr int kErrTimeout = 4;
 
 // Records a failure message for tpm_last_error_message and returns status.
 int fail(int status, const std::string& msg);
@@ -87,12 +88,14 @@ struct tpm_ctx {
   int32_t* prefix = nullptr;  // exclusive scan of the per-level flags (n + 1)
   int32_t* slot = nullptr;    // partner positions of right-misplaced elements
   int32_t* blocksum = nullptr;
+  unsigned long long* scan_status = nullptr;  // look-back words, one per scan tile
   int32_t* cell_count = nullptr;
   int32_t* cell_begin = nullptr;  // C^3 + 1
   uint32_t* thr = nullptr;        // per-dim split thresholds, C + 1
   tpm::TreeNode* tree = nullptr;  // [C * kMaxTreeDepth]
   int* depth1d = nullptr;         // [C]
   int max_depth1d = 0;
+  uint64_t scan_stamp = 0;  // distinguishes look-back status words of successive scans
 
   // mesh
   float* rho = nullptr;  // N^3 real grid (deposit out, r2c in)
@@ -102,7 +105,6 @@ struct tpm_ctx {
   float* k2tab = nullptr;  // k^2 per index, N
   cufftHandle plan_r2c = 0, plan_c2r = 0;
   bool plans = false;
-  int deposit_tile = 8;
 
   // ewald scratch
   double* ew_buf = nullptr;
