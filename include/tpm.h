@@ -46,7 +46,7 @@ extern "C" {
 #define TPM_ERR_TIMEOUT (-9)       /* a bounded device wait gave up */
 #define TPM_ERR_NOEXT (-10)        /* library built without a required part */
 
-/* gravity_long_type (tigerpm/gravity_long.hpp:13-15) */
+/* gravity_long_type (tigerpm/gravity_long.hpp:17-19) */
 #define TPM_GRAVITY_LONG_PM 0
 #define TPM_GRAVITY_LONG_PME 1
 
