@@ -232,6 +232,26 @@ int tpm_gravity_short_ewald(tpm_ctx* ctx, int64_t ns, const uint32_t* sx, const 
 int tpm_ewald_fp64(tpm_ctx* ctx, int64_t ns, const int64_t* sample_idx, int method,
                    double* phi, double* gx, double* gy, double* gz);
 
+/* The same FP64 Ewald sum (method 1) for callers that cannot allocate device
+ * memory, e.g. a host that hands out every byte of device memory from its own
+ * pool, or an allocation-free hook inside a running simulation step.  No
+ * counterpart in the reference.  Sources (x, y, z: n particles), sinks
+ * (sx, sy, sz: ns points) and outputs (phi, gx, gy, gz: ns each) are device
+ * arrays; no context is needed.  All scratch lives in one fixed 448 KiB buffer
+ * inside the library that every GPU loading it keeps until exit; no call
+ * allocates or frees device memory.  ns above TPM_EWALD_NOALLOC_MAX_SINKS is
+ * rejected with TPM_ERR_INVALID.  The first call on a device looks up that
+ * buffer's address and copies a small table into it synchronously, so make
+ * it before any stream capture.  Calls share the buffer: calls that may
+ * overlap on the GPU (other streams or host threads) race and must be
+ * serialised by the caller.  Work is queued on `stream` (NULL: the legacy
+ * default stream); results are ready when that stream is. */
+#define TPM_EWALD_NOALLOC_MAX_SINKS 4096
+int tpm_ewald_fp64_noalloc(const uint32_t* x, const uint32_t* y, const uint32_t* z, int64_t n,
+                           const uint32_t* sx, const uint32_t* sy, const uint32_t* sz, int64_t ns,
+                           double hsoft, double* phi, double* gx, double* gy, double* gz,
+                           void* stream);
+
 /* Average device time per call of each stage over the calls since the last
  * tpm_reset_stage_times (up to the last 64 calls per stage). */
 int tpm_get_stage_times(tpm_ctx* ctx, tpm_stage_times* out);

@@ -1,0 +1,67 @@
+"""tpm_ewald_fp64_noalloc: the FP64 Ewald sum for callers that may not allocate
+device memory (a host that owns all device memory through its own pool, or an
+allocation-free hook inside a running step).  Its scratch is a fixed buffer
+inside the library, so the test checks that two calls in a row -- the second
+on different sinks, over whatever the first left in that buffer -- agree with
+tpm_gravity_short_ewald (method 1), which uses freshly allocated scratch.
+
+This file is collected last on purpose: a run that stops at the first failure
+has run every other test before it."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from helpers import particle_set, rel_rms
+from tigerpm_b200 import _lib
+from tigerpm_b200 import workloads as W
+from tigerpm_b200.api import TigerPM, make_options
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_noalloc_ewald_matches_allocating_path_twice():
+    import torch
+    lib = _lib.load()
+    ps = particle_set("halos", 20, 41)
+    opts = make_options(20, 20, rs_cells=1.0)
+    ref = []
+    sinks = []
+    with TigerPM(opts, ps.n) as t:
+        t.set_particles(ps)
+        for seed in (3, 4):
+            idx = W.sample_indices(ps.n, 96 if seed == 3 else 40, seed)
+            sx, sy, sz = ps.x[idx].copy(), ps.y[idx].copy(), ps.z[idx].copy()
+            sx[0] = sx[0] + 777  # a near pair that is not the sink itself
+            phi, g = t.gravity_short_ewald_call_kernel(sx, sy, sz, method=1)
+            ref.append((phi, np.stack(g, 1)))
+            sinks.append((sx, sy, sz))
+    x, y, z = (_dev(torch, a) for a in (ps.x, ps.y, ps.z))
+    stream = torch.cuda.current_stream().cuda_stream
+    for (sx, sy, sz), (rphi, rg) in zip(sinks, ref):
+        ns = sx.size
+        dsx, dsy, dsz = (_dev(torch, a) for a in (sx, sy, sz))
+        out = [torch.full((ns,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(4)]
+        rc = lib.tpm_ewald_fp64_noalloc(C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                        C.c_void_p(z.data_ptr()), ps.n, C.c_void_p(dsx.data_ptr()),
+                                        C.c_void_p(dsy.data_ptr()), C.c_void_p(dsz.data_ptr()), ns, opts.hsoft,
+                                        *[C.c_void_p(o.data_ptr()) for o in out], C.c_void_p(stream))
+        _lib.check(rc, "tpm_ewald_fp64_noalloc")
+        torch.cuda.synchronize()
+        phi = out[0].cpu().numpy()
+        g = torch.stack(out[1:], 1).cpu().numpy()
+        assert np.all(np.isfinite(phi)) and np.all(np.isfinite(g))
+        assert rel_rms(phi, rphi) < 1e-9
+        assert rel_rms(g, rg) < 1e-9
+
+
+def test_noalloc_ewald_rejects_too_many_sinks():
+    lib = _lib.load()
+    rc = lib.tpm_ewald_fp64_noalloc(None, None, None, 0, None, None, None, _lib.TPM_EWALD_NOALLOC_MAX_SINKS + 1,
+                                    0.01, None, None, None, None, None)
+    assert rc == _lib.TPM_ERR_INVALID
+    assert b"exceed its maximum" in lib.tpm_last_error_message()

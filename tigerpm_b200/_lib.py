@@ -23,6 +23,7 @@ TPM_ERR_CAPACITY = -7
 TPM_ERR_BUDGET = -8
 TPM_ERR_TIMEOUT = -9
 TPM_ERR_NOEXT = -10
+TPM_EWALD_NOALLOC_MAX_SINKS = 4096
 
 GRAVITY_LONG_PM = 0
 GRAVITY_LONG_PME = 1
@@ -91,6 +92,7 @@ SIGNATURES = [
     ("tpm_drift", _I, [_P, _D]),
     ("tpm_gravity_short_ewald", _I, [_P, _I64, _P, _P, _P, _I, _P, _P, _P, _P]),
     ("tpm_ewald_fp64", _I, [_P, _I64, _P, _I, _P, _P, _P, _P]),
+    ("tpm_ewald_fp64_noalloc", _I, [_P, _P, _P, _I64, _P, _P, _P, _I64, _D, _P, _P, _P, _P, _P]),
     ("tpm_get_stage_times", _I, [_P, C.POINTER(StageTimes)]),
     ("tpm_reset_stage_times", _I, [_P]),
     ("tpm_get_launch_count", _I, [_P, C.POINTER(_I64)]),
