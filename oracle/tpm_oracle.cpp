@@ -253,12 +253,34 @@ struct Fft1D {
     }
   }
 
+  // n = p * 2^k with p in {3, 5}: one radix-p stage over p power-of-two
+  // transforms (direct, no Bluestein).
+  int radix = 1;
+  int sub = 0;
+  std::vector<cd> tw_sub, tw_n;
+
   void init(int n_) {
     n = n_;
     pow2 = (n & (n - 1)) == 0;
     if (pow2) {
       make_tw(n, tw);
       return;
+    }
+    for (int p : {3, 5}) {
+      if (n % p == 0) {
+        const int q = n / p;
+        if ((q & (q - 1)) == 0) {
+          radix = p;
+          sub = q;
+          make_tw(q, tw_sub);
+          tw_n.resize(n);
+          for (int k = 0; k < n; k++) {
+            const double a = -2.0 * M_PI * k / n;
+            tw_n[k] = cd(std::cos(a), std::sin(a));
+          }
+          return;
+        }
+      }
     }
     m = 1;
     while (m < 2 * n - 1) m <<= 1;
@@ -282,6 +304,26 @@ struct Fft1D {
   void exec(cd* a, int sign, std::vector<cd>& scratch) const {
     if (pow2) {
       radix2(a, n, tw, sign);
+      return;
+    }
+    if (radix > 1) {
+      // X[k] = sum_r W_n^{r k} F_r[k mod q], F_r = FFT_q of a[p j + r]
+      const int p = radix, q = sub;
+      scratch.resize(n);
+      for (int r = 0; r < p; r++) {
+        cd* f = scratch.data() + r * q;
+        for (int j = 0; j < q; j++) f[j] = a[p * j + r];
+        radix2(f, q, tw_sub, sign);
+      }
+      for (int k = 0; k < n; k++) {
+        cd acc = scratch[k % q];
+        for (int r = 1; r < p; r++) {
+          cd w = tw_n[(int)(((long long)r * k) % n)];
+          if (sign > 0) w = std::conj(w);
+          acc += w * scratch[r * q + k % q];
+        }
+        a[k] = acc;
+      }
       return;
     }
     // Backward transform = conj(forward(conj(a))).
