@@ -195,6 +195,13 @@ int tpm_gravity_long_compute(tpm_ctx* ctx, int type);
  * {b0,b1,b2,e0,e1,e2} (any integer box; indices wrap periodically), written
  * x-major / z fastest as range<int>::index orders it (tigerpm/range.hpp:149-165). */
 int tpm_gravity_long_get_phi(tpm_ctx* ctx, const int box[6], float* out);
+/* Loads an externally computed periodic potential: four_dim^3 host floats,
+ * x-major / z fastest, in the units gravity_long_compute produces.  The
+ * reference's kick_pme takes its potential through gravity_long_get_phi
+ * (src/kick_pme.cu:446); a caller that keeps its own long-range solver hands
+ * that potential to tpm_kick_pme this way.  Valid until the next drift or
+ * set_particles. */
+int tpm_gravity_long_set_phi(tpm_ctx* ctx, const float* phi);
 /* gravity_long_get_phi_box (src/gravity_long.cpp:19-21): the PHI_BW-padded
  * source box of this rank. */
 int tpm_gravity_long_get_phi_box(const tpm_ctx* ctx, int box[6]);

@@ -63,6 +63,8 @@ def lib():
     L.orc_erfcexp.restype = C.c_float
     L.orc_erfcexp.argtypes = [C.c_float, C.POINTER(C.c_float)]
     L.orc_fixed32_from_double_array.argtypes = [C.c_int64, f64p, u32p]
+    L.orc_fixed32_convert_array.argtypes = [C.c_int64, u32p, u32p, f32p, f64p, f32p]
+    L.orc_cloud4_array.argtypes = [C.c_int64, f64p, f64p]
     L.orc_mesh_loc.argtypes = [C.c_int, C.c_int64, u32p, i32p]
     L.orc_chainmesh_sort.restype = C.c_int
     L.orc_chainmesh_sort.argtypes = [C.c_int, C.c_int64, u32p, u32p, u32p, f32p, f32p, f32p,
@@ -107,6 +109,32 @@ def fixed32_to_double(i: int) -> float:
 def distance(a: int, b: int) -> float:
     """distance(fixed32, fixed32) (tigerpm/gravity_short.hpp:20-22)."""
     return float(lib().orc_distance(int(a), int(b)))
+
+
+def fixed32_from_double_array(x) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.float64)
+    out = np.empty(x.size, np.uint32)
+    lib().orc_fixed32_from_double_array(x.size, x, out)
+    return out
+
+
+def fixed32_convert_array(a, b):
+    """(to_float(a), to_double(a), distance(a, b)) elementwise."""
+    a = np.ascontiguousarray(a, np.uint32)
+    b = np.ascontiguousarray(b, np.uint32)
+    tf = np.empty(a.size, np.float32)
+    td = np.empty(a.size, np.float64)
+    ds = np.empty(a.size, np.float32)
+    lib().orc_fixed32_convert_array(a.size, a, b, tf, td, ds)
+    return tf, td, ds
+
+
+def cloud4(x) -> np.ndarray:
+    """cloud4 (src/gravity_long.cpp:127-138)."""
+    x = np.ascontiguousarray(x, np.float64)
+    out = np.empty(x.size, np.float64)
+    lib().orc_cloud4_array(x.size, x, out)
+    return out
 
 
 def erfcexp(x: float):

@@ -485,6 +485,21 @@ void orc_fixed32_from_double_array(int64_t n, const double* x, uint32_t* out) {
   for (int64_t i = 0; i < n; i++) out[i] = fixed_from_double(x[i]);
 }
 
+// Array forms of the conversions and of distance(), for the golden-vector checks.
+void orc_fixed32_convert_array(int64_t n, const uint32_t* a, const uint32_t* b, float* to_float,
+                               double* to_double, float* dist) {
+  for (int64_t i = 0; i < n; i++) {
+    to_float[i] = fixed_to_float(a[i]);
+    to_double[i] = fixed_to_double(a[i]);
+    dist[i] = distance32(a[i], b[i]);
+  }
+}
+
+// cloud4 (src/gravity_long.cpp:127-138), one value per x.
+void orc_cloud4_array(int64_t n, const double* x, double* w) {
+  for (int64_t i = 0; i < n; i++) w[i] = cloud4(x[i]);
+}
+
 // particles_mesh_loc: i = int(to_double(x) * C) (tigerpm/particles.hpp:60-67).
 void orc_mesh_loc(int C, int64_t n, const uint32_t* x, int32_t* loc) {
   const double Cd = C;

@@ -86,6 +86,7 @@ SIGNATURES = [
     ("tpm_chainmesh_interior_box", _I, [_P, _P]),
     ("tpm_gravity_long_compute", _I, [_P, _I]),
     ("tpm_gravity_long_get_phi", _I, [_P, _P, _P]),
+    ("tpm_gravity_long_set_phi", _I, [_P, _P]),
     ("tpm_gravity_long_get_phi_box", _I, [_P, _P]),
     ("tpm_gravity_long_force_at", _I, [_P, _I64, _P, _P, _P]),
     ("tpm_kick_pme", _I, [_P, _P, _I, _D, _D, _I]),

@@ -221,6 +221,14 @@ class TigerPM:
         check(self.lib.tpm_gravity_long_get_phi(self.h, box.as_array(), _ptr(out)), "gravity_long_get_phi")
         return out.reshape(box.shape())
 
+    def gravity_long_set_phi(self, phi: np.ndarray) -> None:
+        """Load a periodic four_dim^3 potential (x-major, z fastest) computed
+        elsewhere; kick_pme then uses it as gravity_long_get_phi's result."""
+        a = np.ascontiguousarray(phi, np.float32)
+        if a.size != self.opts.four_dim ** 3:
+            raise ValueError("phi must hold four_dim^3 values")
+        check(self.lib.tpm_gravity_long_set_phi(self.h, _ptr(a)), "gravity_long_set_phi")
+
     def gravity_long_get_phi_box(self) -> Range:
         b = (C.c_int * 6)()
         check(self.lib.tpm_gravity_long_get_phi_box(self.h, b), "gravity_long_get_phi_box")

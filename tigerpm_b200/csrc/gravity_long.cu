@@ -382,6 +382,15 @@ int gravity_long_get_phi(tpm_ctx* c, const int box[6], float* out) {
   return TPM_OK;
 }
 
+int gravity_long_set_phi(tpm_ctx* c, const float* phi) {
+  const size_t bytes = sizeof(float) * (size_t)c->N * c->N * c->N;
+  cudaError_t e = cudaMemcpyAsync(c->phi, phi, bytes, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return fail(TPM_ERR_CUDA, std::string("set_phi: ") + cudaGetErrorString(e));
+  c->have_phi = true;
+  return TPM_OK;
+}
+
 int gravity_long_force_at(tpm_ctx* c, int64_t n, const double* pos, float* phi_out, float* g_out) {
   if (!c->have_phi) return fail(TPM_ERR_STATE, "gravity_long_force_at needs gravity_long_compute first");
   if (n <= 0) return TPM_OK;

@@ -507,6 +507,11 @@ int tpm_gravity_long_get_phi(tpm_ctx* c, const int box[6], float* out) {
   return gravity_long_get_phi(c, box, out);
 }
 
+int tpm_gravity_long_set_phi(tpm_ctx* c, const float* phi) {
+  if (!c || !phi) return fail(TPM_ERR_INVALID, "null argument");
+  return gravity_long_set_phi(c, phi);
+}
+
 int tpm_gravity_long_get_phi_box(const tpm_ctx* c, int box[6]) {
   if (!c || !box) return fail(TPM_ERR_INVALID, "null argument");
   // source_box = chain box * four_o_chain padded by PHI_BW (src/gravity_long.cpp:150-156);

@@ -127,6 +127,7 @@ void stage_end(tpm_ctx* c, Stage s);
 int chainmesh_sort(tpm_ctx* c);
 int gravity_long(tpm_ctx* c, int type);
 int gravity_long_get_phi(tpm_ctx* c, const int box[6], float* out);
+int gravity_long_set_phi(tpm_ctx* c, const float* phi);
 int gravity_long_force_at(tpm_ctx* c, int64_t n, const double* pos, float* phi, float* g);
 int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0, int first_call);
 int drift(tpm_ctx* c, double dt);
