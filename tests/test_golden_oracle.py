@@ -11,10 +11,13 @@ sources (oracle/build_ref.sh) and run by tests/golden/make_golden.py.
               the oracle works in FP64, so within FP32 rounding (2e-6 relative)
   kick_*      kick_pme_kernel on a B200 (src/kick_pme.cu:128-357), given the
               same sorted particles, cell table and potential: the oracle's
-              FP32 path within 2e-5 relative RMS (libm vs CUDA's erfc/exp/rsqrt
-              and summation order), rungs identical but for power-of-two ties
+              FP32 path within 5e-6 relative RMS (measured 2e-7..5e-7: libm vs
+              CUDA's sqrt/rsqrt and summation order), rungs identical but for
+              power-of-two ties
   ewald_*     gravity_ewald_kernel on a B200 (src/gravity_short.cu:93-201):
-              the oracle's restatement within 1e-5 relative RMS
+              the oracle's restatement within 1e-5 relative RMS (measured
+              1e-7 on forces, 2e-6 on the uniform case's potential, where
+              the sum cancels)
 """
 import numpy as np
 import pytest
@@ -77,8 +80,8 @@ def test_kick(case):
     assert active.any()
     G = np.stack([gx, gy, gz], 1)[active]
     RG = np.stack([d["out_gx"], d["out_gy"], d["out_gz"]], 1)[active]
-    assert rel_rms(G, RG) < 2e-5
-    assert rel_rms(pot[active], d["out_pot"][active]) < 2e-5
+    assert rel_rms(G, RG) < 5e-6
+    assert rel_rms(pot[active], d["out_pot"][active]) < 5e-6
     assert np.mean(p.rung != d["out_rung"]) < 2e-3
     assert np.abs(p.rung.astype(int) - d["out_rung"].astype(int)).max() <= 1
     # inactive sinks are untouched by both

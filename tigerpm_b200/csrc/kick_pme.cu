@@ -133,9 +133,18 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
   lp = sp;
 }
 
-// One source against one sink (src/kick_pme.cu:285-314).
+// One source against one sink (src/kick_pme.cu:285-314).  WRAP folds the
+// offset to the minimum image, as the reference's int32 difference does; it
+// is needed only when chain_dim = 3, where the 27 cells span the whole box
+// and an offset from the cell centre can exceed half the box.
+template <bool WRAP>
 __device__ __forceinline__ void pair(const KickArgs& a, float dx, float dy, float dz, float& gx, float& gy,
                                      float& gz, float& ph) {
+  if (WRAP) {
+    dx -= rintf(dx);
+    dy -= rintf(dy);
+    dz -= rintf(dz);
+  }
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   const float r2c = fmaxf(r2, a.h2);
   const float rinv = rsqrt_approx(r2c);
@@ -197,6 +206,7 @@ constexpr int kGroup = 8;
 constexpr int kBuf = 64;
 constexpr int kMaxRuns = 18;
 
+template <bool WRAP>
 __global__ void __launch_bounds__(kKickThreads, 2) k_kick_pme(KickArgs a, int stage) {
   extern __shared__ float4 smem4[];
   const int T = blockDim.x, W = T >> 5;
@@ -223,7 +233,7 @@ __global__ void __launch_bounds__(kKickThreads, 2) k_kick_pme(KickArgs a, int st
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int t8 = lane & 7, ph = lane >> 3;
   const float Cf = (float)C;
-  const bool cull = a.rcut2 < INFINITY;
+  const bool cull = !WRAP && a.rcut2 < INFINITY;  // culling works on unwrapped offsets
   if (tid == 0) {
     int nr = 0, tot = 0;
     for (int dz = -1; dz <= 1; dz++) {
@@ -352,7 +362,7 @@ __global__ void __launch_bounds__(kKickThreads, 2) k_kick_pme(KickArgs a, int st
 #pragma unroll
             for (int k = 0; k < 32; k += 4) {
               const float4 u = buf[k + ph];
-              if (mysink) pair(a, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
+              if (mysink) pair<WRAP>(a, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
             }
             __syncwarp();
             if (lane < cnt - 32) buf[lane] = buf[32 + lane];
@@ -363,7 +373,7 @@ __global__ void __launch_bounds__(kKickThreads, 2) k_kick_pme(KickArgs a, int st
         for (int k = 0; k < cnt; k += 4) {
           if (k + ph < cnt && mysink) {
             const float4 u = buf[k + ph];
-            pair(a, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
+            pair<WRAP>(a, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
           }
         }
         __syncwarp();
@@ -497,10 +507,12 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
   stage = (stage + 127) / 128 * 128;
   const size_t smem = sizeof(float4) * ((size_t)stage + (size_t)W * kBuf + kPass) + sizeof(float) * kPass * 8 +
                       sizeof(unsigned) * kPass + sizeof(int) * (2 * kMaxRuns + 2);
-  TPM_CUDA_TRY(cudaFuncSetAttribute(k_kick_pme, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const bool wrap = C == 3;
+  auto kern = wrap ? k_kick_pme<true> : k_kick_pme<false>;
+  TPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   stage_begin(c, kStKick);
   if (ncell > 0) {
-    k_kick_pme<<<(unsigned)ncell, T, smem, c->stream>>>(a, stage);
+    kern<<<(unsigned)ncell, T, smem, c->stream>>>(a, stage);
     c->launches++;
     TPM_CUDA_TRY(cudaGetLastError());
   }

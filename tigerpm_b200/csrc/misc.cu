@@ -51,7 +51,12 @@ __global__ void __launch_bounds__(256) k_count_pairs(const int4* __restrict__ po
               cand += len;
               for (int j = 0; j < len; j++) {
                 const float4 s = src[j];
-                const float ddx = sx - s.x, ddy = sy - s.y, ddz = sz - s.z;
+                float ddx = sx - s.x, ddy = sy - s.y, ddz = sz - s.z;
+                if (C == 3) {  // minimum image, as in the kick
+                  ddx -= rintf(ddx);
+                  ddy -= rintf(ddy);
+                  ddz -= rintf(ddz);
+                }
                 in += fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz)) < rcut2 ? 1 : 0;
               }
             }
