@@ -15,6 +15,9 @@ Workloads (synthetic, seeded Philox; see tigerpm_b200/workloads.py):
                r_s = 2 mesh cells, cutoff 6 r_s: the form of the 256^3
                configuration that meets rms force error <= 1e-4 at the lowest
                measured step time (TSC and the literal r_s / mesh do not).
+  c2-accurate-128  the same form at 128^3 particles / 384^3 mesh: the same
+               chain-cell occupancy (64 per cell) and kernel shapes, an eighth of
+               the work; the small case the ncu captures run on.
   c2           the same particles with the configuration's literal mesh
                parameters: 256^3 mesh, TSC, r_s = 1.25 cells, cutoff 4.5 r_s.
   c1           64^3 uniform particles, 64^3 mesh, CIC, r_s 1.25, 4.5 r_s.
@@ -45,6 +48,8 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     "c2-accurate": dict(kind="zeldovich", n_side=256, grid=768, assign="cloud4", rs_cells=2.0, rcut_over_rs=6.0,
                         ewald_samples=4096),
+    "c2-accurate-128": dict(kind="zeldovich", n_side=128, grid=384, assign="cloud4", rs_cells=2.0, rcut_over_rs=6.0,
+                            ewald_samples=4096),
     "c2": dict(kind="zeldovich", n_side=256, grid=256, assign="tsc", rs_cells=1.25, rcut_over_rs=4.5,
                ewald_samples=4096),
     "c1": dict(kind="uniform", n_side=64, grid=64, assign="cic", rs_cells=1.25, rcut_over_rs=4.5,

@@ -109,6 +109,7 @@ typedef struct tpm_stage_times {
   float kick_ms;
   float drift_ms;
   float ewald_ms;
+  float interp_ms; /* long-range interpolation at the sinks (part of the kick) */
 } tpm_stage_times;
 
 /* Device addresses of the context's particle arrays (current order). */

@@ -100,3 +100,20 @@ def test_fast_order(kind, n_side, C):
     for c in range(C ** 3):  # stable: ascending input index inside each cell
         seg = idx[offsets[c]:offsets[c + 1]]
         assert np.all(np.diff(seg) > 0)
+
+
+def test_parity_dense_clump():
+    """A dense clump (24,000 particles in one chain cell) among 40,000 uniform
+    ones: deep recursion nodes far larger than the mean."""
+    C = 6
+    ps = W.uniform(64000, 17)
+    g = W.rng(18)
+    k = 24000
+    for a in (ps.x, ps.y, ps.z):
+        a[:k] = (g.integers(0, 2 ** 32 // C, k, dtype=np.uint64) + 2 * (2 ** 32 // C)).astype(np.uint32)
+    ps = with_random_motion(ps, 17)
+    (x, y, z, vx, vy, vz, r), offsets, _ = run_device(ps, C)
+    p, pb, pe = run_oracle(ps, C)
+    assert np.array_equal(x, p.x) and np.array_equal(y, p.y) and np.array_equal(z, p.z)
+    assert np.array_equal(r, p.rung)
+    assert np.array_equal(offsets[:-1], pb) and np.array_equal(offsets[1:], pe)

@@ -49,7 +49,8 @@ class Options(C.Structure):
 
 class StageTimes(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("sort_ms", "deposit_ms", "fft_forward_ms", "green_ms",
-                                         "fft_inverse_ms", "kick_ms", "drift_ms", "ewald_ms")]
+                                         "fft_inverse_ms", "kick_ms", "drift_ms", "ewald_ms",
+                                         "interp_ms")]
 
 
 class DeviceArrays(C.Structure):

@@ -35,6 +35,21 @@ namespace tpm {
 namespace {
 
 constexpr int kKickThreads = 256;
+// Occupancy settings, measured on B200 at 64 particles per chain cell
+// (256^3 particles, 64^3 cells): 64 registers (4 resident 256-thread blocks
+// per SM), a staged chunk of half the mean 27-cell neighbourhood and a sink
+// pass of the power of two >= the mean cell give 8 resident 128-thread
+// blocks and the shortest kick (18.8 ms; 26.9 ms at 80 registers and 4 blocks,
+// 20.9 ms at 48 or 40 registers, where the pair loop loses ILP).
+#ifndef TPM_KICK_MINB
+#define TPM_KICK_MINB 4  // resident 256-thread blocks per SM the register budget targets
+#endif
+#ifndef TPM_KICK_STAGE_X100
+#define TPM_KICK_STAGE_X100 50  // staged sources per chunk, in hundredths of the mean 27-cell neighbourhood
+#endif
+#ifndef TPM_KICK_PASS_X
+#define TPM_KICK_PASS_X 1  // 0: 256 sinks per pass; k: the power of two >= k x the mean cell, 64..256
+#endif
 constexpr int kMaxStage = 4096;  // sources staged per chunk (64 KB)
 
 struct KickArgs {
@@ -48,6 +63,7 @@ struct KickArgs {
   float* __restrict__ gz;
   float* __restrict__ pot;
   const int32_t* __restrict__ begin;
+  const uint32_t* __restrict__ thr;  // chain-cell split thresholds (C + 1)
   const float* __restrict__ phi;
   int* __restrict__ err;
   int C, N;
@@ -133,6 +149,136 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
   lp = sp;
 }
 
+// Long-range part at every active sink of the kick box, stored in gx/gy/gz/pot
+// (unscaled); k_kick_pme adds the pair sums and applies GM.  Two kernels
+// compute it, one block per sink cell, chosen by the mesh points per sink.
+//
+// Direct form: one thread per sink, the 216 points read through L1.
+__global__ void __launch_bounds__(64) k_interp_direct(KickArgs a) {
+  int bid = blockIdx.x;
+  const int i2 = bid % a.s2;
+  bid /= a.s2;
+  const int i1 = bid % a.s1;
+  const int i0 = bid / a.s1;
+  const int C = a.C;
+  const int64_t key = ((int64_t)(a.b2 + i2) * C + (a.b1 + i1)) * C + (a.b0 + i0);
+  const int32_t pb = __ldg(a.begin + key), pe = __ldg(a.begin + key + 1);
+  for (int32_t i = pb + (int32_t)threadIdx.x; i < pe; i += blockDim.x) {
+    if (a.rung[i] < a.min_rung) continue;
+    float lx, ly, lz, lp;
+    interp_long(a, __ldg(a.pos4 + i), lx, ly, lz, lp);
+    a.gx[i] = lx;
+    a.gy[i] = ly;
+    a.gz[i] = lz;
+    a.pot[i] = lp;
+  }
+}
+
+// The same interpolation from a shared-memory copy of the potential: one
+// block per sink cell stages the mesh points every sink of the cell can
+// reach (the cell's mesh span plus the stencil's 2 + 3 points per dim),
+// then each sink reads its 6^3 points from the tile.  Blocks whose span
+// exceeds the tile take the direct path.
+__device__ __forceinline__ void interp_tile(const float* __restrict__ tile, int W0, int W1, int W2, int bx, int by,
+                                            int bz, int4 q, int N, float& lx, float& ly, float& lz, float& lp) {
+  float w[3][kNInterp], dw[3][kNInterp];
+  const uint32_t r[3] = {(uint32_t)q.x, (uint32_t)q.y, (uint32_t)q.z};
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const uint64_t t = (uint64_t)r[d] * (uint64_t)N;
+    base[d] = (int)(t >> 32) - 2;
+    q6((float)(uint32_t)t * 2.3283064365386963e-10f, w[d], dw[d]);
+  }
+  // sinks of the cell lie inside the tile by construction; the clamp keeps a
+  // stale (moved, unsorted) particle inside it as well
+  const int ox = min(max(base[0] - bx, 0), W0 - kNInterp);
+  const int oy = min(max(base[1] - by, 0), W1 - kNInterp);
+  const int oz = min(max(base[2] - bz, 0), W2 - kNInterp);
+  float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+  for (int i = 0; i < kNInterp; i++) {
+    const float* plane = tile + (ox + i) * W1 * W2 + oy * W2 + oz;
+    float px = 0.f, py = 0.f, pz = 0.f;
+#pragma unroll
+    for (int j = 0; j < kNInterp; j++) {
+      float rz = 0.f, rdz = 0.f;
+#pragma unroll
+      for (int k = 0; k < kNInterp; k++) {
+        const float v = plane[j * W2 + k];
+        rz = fmaf(w[2][k], v, rz);
+        rdz = fmaf(dw[2][k], v, rdz);
+      }
+      px = fmaf(w[1][j], rz, px);
+      py = fmaf(dw[1][j], rz, py);
+      pz = fmaf(w[1][j], rdz, pz);
+    }
+    sx = fmaf(dw[0][i], px, sx);
+    sy = fmaf(w[0][i], py, sy);
+    sz = fmaf(w[0][i], pz, sz);
+    sp = fmaf(w[0][i], px, sp);
+  }
+  lx = -sx * (float)N;
+  ly = -sy * (float)N;
+  lz = -sz * (float)N;
+  lp = sp;
+}
+
+__global__ void __launch_bounds__(128) k_interp_tile(KickArgs a, int maxw) {
+  extern __shared__ float tile[];
+  int bid = blockIdx.x;
+  const int i2 = bid % a.s2;
+  bid /= a.s2;
+  const int i1 = bid % a.s1;
+  const int i0 = bid / a.s1;
+  const int C = a.C, N = a.N;
+  const int cc[3] = {a.b0 + i0, a.b1 + i1, a.b2 + i2};
+  const int64_t key = ((int64_t)cc[2] * C + cc[1]) * C + cc[0];
+  const int32_t pb = __ldg(a.begin + key), pe = __ldg(a.begin + key + 1);
+  if (pb == pe) return;
+  int o[3], W[3];
+  bool fits = true;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const uint32_t lo_r = __ldg(a.thr + cc[d]);
+    const uint32_t hi_r = cc[d] + 1 < C ? __ldg(a.thr + cc[d] + 1) - 1u : 0xffffffffu;
+    const int lo = (int)(((uint64_t)lo_r * (uint64_t)N) >> 32);
+    const int hi = (int)(((uint64_t)hi_r * (uint64_t)N) >> 32);
+    o[d] = lo - 2;
+    W[d] = hi - lo + 6;
+    fits = fits && W[d] <= maxw;
+  }
+  if (!fits) {  // uniform per block
+    for (int32_t i = pb + (int32_t)threadIdx.x; i < pe; i += blockDim.x) {
+      if (a.rung[i] < a.min_rung) continue;
+      float lx, ly, lz, lp;
+      interp_long(a, __ldg(a.pos4 + i), lx, ly, lz, lp);
+      a.gx[i] = lx;
+      a.gy[i] = ly;
+      a.gz[i] = lz;
+      a.pot[i] = lp;
+    }
+    return;
+  }
+  const int plane = W[1] * W[2];
+  const int vol = W[0] * plane;
+  for (int t = threadIdx.x; t < vol; t += blockDim.x) {
+    const int u = t / plane, r = t - u * plane;
+    const int v = r / W[2], w = r - v * W[2];
+    const int64_t g = ((int64_t)wrapi(o[0] + u, N) * N + wrapi(o[1] + v, N)) * N + wrapi(o[2] + w, N);
+    tile[t] = __ldg(a.phi + g);
+  }
+  __syncthreads();
+  for (int32_t i = pb + (int32_t)threadIdx.x; i < pe; i += blockDim.x) {
+    if (a.rung[i] < a.min_rung) continue;
+    float lx, ly, lz, lp;
+    interp_tile(tile, W[0], W[1], W[2], o[0], o[1], o[2], __ldg(a.pos4 + i), N, lx, ly, lz, lp);
+    a.gx[i] = lx;
+    a.gy[i] = ly;
+    a.gz[i] = lz;
+    a.pot[i] = lp;
+  }
+}
+
 // One source against one sink (src/kick_pme.cu:285-314).  WRAP folds the
 // offset to the minimum image, as the reference's int32 difference does; it
 // is needed only when chain_dim = 3, where the 27 cells span the whole box
@@ -207,15 +353,15 @@ constexpr int kBuf = 64;
 constexpr int kMaxRuns = 18;
 
 template <bool WRAP>
-__global__ void __launch_bounds__(kKickThreads, 2) k_kick_pme(KickArgs a, int stage) {
+__global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickArgs a, int stage, int npass) {
   extern __shared__ float4 smem4[];
   const int T = blockDim.x, W = T >> 5;
   float4* src = smem4;
   float4* bufs = src + stage;
   float4* spos = bufs + W * kBuf;
-  float* acc = reinterpret_cast<float*>(spos + kPass);
-  unsigned* skey = reinterpret_cast<unsigned*>(acc + kPass * 8);
-  int* runb = reinterpret_cast<int*>(skey + kPass);
+  float* acc = reinterpret_cast<float*>(spos + npass);
+  unsigned* skey = reinterpret_cast<unsigned*>(acc + npass * 8);
+  int* runb = reinterpret_cast<int*>(skey + npass);
   int* runp = runb + kMaxRuns;
   const int C = a.C;
   int bid = blockIdx.x;
@@ -263,10 +409,10 @@ __global__ void __launch_bounds__(kKickThreads, 2) k_kick_pme(KickArgs a, int st
   __syncthreads();
   const int total = runp[kMaxRuns];
   float4* buf = bufs + warp * kBuf;
-  for (int32_t sbase = pb; sbase < pe; sbase += kPass) {
+  for (int32_t sbase = pb; sbase < pe; sbase += npass) {
     // 1. order this pass's active sinks by sub-cell (deterministic bitonic sort)
-    if (tid == 0) runp[kMaxRuns + 1] = kPass;  // active count when every slot is active
-    for (int e = tid; e < kPass; e += T) {
+    if (tid == 0) runp[kMaxRuns + 1] = npass;  // active count when every slot is active
+    for (int e = tid; e < npass; e += T) {
       const int32_t i = sbase + e;
       unsigned k = 512u;  // inactive / absent sinks sort last
       if (i < pe && a.rung[i] >= a.min_rung) {
@@ -276,9 +422,9 @@ __global__ void __launch_bounds__(kKickThreads, 2) k_kick_pme(KickArgs a, int st
       skey[e] = (k << 8) | (unsigned)e;
     }
     __syncthreads();
-    for (int kk = 2; kk <= kPass; kk <<= 1) {
+    for (int kk = 2; kk <= npass; kk <<= 1) {
       for (int j = kk >> 1; j > 0; j >>= 1) {
-        for (int e = tid; e < kPass; e += T) {
+        for (int e = tid; e < npass; e += T) {
           const int ixj = e ^ j;
           if (ixj > e) {
             const unsigned u = skey[e], v = skey[ixj];
@@ -292,7 +438,7 @@ __global__ void __launch_bounds__(kKickThreads, 2) k_kick_pme(KickArgs a, int st
         __syncthreads();
       }
     }
-    for (int e = tid; e < kPass; e += T) {
+    for (int e = tid; e < npass; e += T) {
       const unsigned m = skey[e];
       const bool act = (m >> 8) < 512u;
       float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -405,9 +551,7 @@ __global__ void __launch_bounds__(kKickThreads, 2) k_kick_pme(KickArgs a, int st
     // 2. long-range interpolation and the kick, one thread per sorted sink
     for (int e = tid; e < nact; e += T) {
       const int32_t i = sbase + (int32_t)(skey[e] & 0xffu);
-      const int4 q = __ldg(a.pos4 + i);
-      float lx, ly, lz, lp;
-      interp_long(a, q, lx, ly, lz, lp);
+      const float lx = a.gx[i], ly = a.gy[i], lz = a.gz[i], lp = a.pot[i];  // from k_interp_long
       const float* A = acc + e * 8;
       const float g0 = ((A[0] - A[4]) + lx) * a.GM;
       const float g1 = ((A[1] - A[5]) + ly) * a.GM;
@@ -472,6 +616,7 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
   a.gz = c->gz;
   a.pot = c->pot;
   a.begin = c->cell_begin;
+  a.thr = c->thr;
   a.phi = c->phi;
   a.err = c->d_err;
   a.C = C;
@@ -503,16 +648,41 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
   const double mean_cell = (double)c->n / ((double)C * C * C);
   const int W = (int)std::min(8.0, std::max(2.0, std::ceil(mean_cell / (2.0 * kGroup))));
   const int T = 32 * W;
-  int stage = (int)std::min<double>(kMaxStage, std::max<double>(512.0, 1.25 * 27.0 * mean_cell));
+  int stage = (int)std::min<double>(kMaxStage, std::max<double>(512.0, TPM_KICK_STAGE_X100 * 0.01 * 27.0 * mean_cell));
   stage = (stage + 127) / 128 * 128;
-  const size_t smem = sizeof(float4) * ((size_t)stage + (size_t)W * kBuf + kPass) + sizeof(float) * kPass * 8 +
-                      sizeof(unsigned) * kPass + sizeof(int) * (2 * kMaxRuns + 2);
+  int npass = kPass;
+  if (TPM_KICK_PASS_X > 0) {
+    npass = 64;
+    while (npass < kPass && npass < TPM_KICK_PASS_X * mean_cell) npass *= 2;
+  }
+  const size_t smem = sizeof(float4) * ((size_t)stage + (size_t)W * kBuf + npass) + sizeof(float) * npass * 8 +
+                      sizeof(unsigned) * npass + sizeof(int) * (2 * kMaxRuns + 2);
   const bool wrap = C == 3;
   auto kern = wrap ? k_kick_pme<true> : k_kick_pme<false>;
   TPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // Long-range interpolation.  A shared-memory tile of phi pays when a chain
+  // cell's reach (its mesh span + 5 points per dim) is small against its
+  // sinks (c2: 11.7^3 points for 184 sinks, 3.0 -> 2.1 ms); at 27 mesh cells
+  // per particle (18^3 points for 64 sinks) staging costs more than the direct
+  // reads, which run at the L1 sector limit (3.4 ms at 256^3 on a 768^3 mesh).
+  const int maxw = (c->N + C - 1) / C + 8;
+  const size_t tile_bytes = sizeof(float) * (size_t)maxw * maxw * maxw;
+  const double span = (double)c->N / C + 6.0;
+  const double mean_sinks = (double)c->n / ((double)C * C * C);
+  stage_begin(c, kStInterp);
+  if (ncell > 0) {
+    if (tile_bytes <= 48 * 1024 && span * span * span <= 16.0 * mean_sinks) {
+      k_interp_tile<<<(unsigned)ncell, 128, tile_bytes, c->stream>>>(a, maxw);
+    } else {
+      k_interp_direct<<<(unsigned)ncell, 64, 0, c->stream>>>(a);
+    }
+    c->launches++;
+    TPM_CUDA_TRY(cudaGetLastError());
+  }
+  stage_end(c, kStInterp);
   stage_begin(c, kStKick);
   if (ncell > 0) {
-    kern<<<(unsigned)ncell, T, smem, c->stream>>>(a, stage);
+    kern<<<(unsigned)ncell, T, smem, c->stream>>>(a, stage, npass);
     c->launches++;
     TPM_CUDA_TRY(cudaGetLastError());
   }

@@ -247,7 +247,7 @@ int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out) {
     delete c;
     return fail(TPM_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
   }
-  for (int s = 0; s < 8; s++) {
+  for (int s = 0; s < kNumStages; s++) {
     for (int k = 0; k < kStageSlots; k++) {
       cudaEventCreate(&c->ev.beg[s][k]);
       cudaEventCreate(&c->ev.end[s][k]);
@@ -329,7 +329,7 @@ int tpm_ctx_destroy(tpm_ctx* c) {
     cufftDestroy(c->plan_r2c);
     cufftDestroy(c->plan_c2r);
   }
-  for (int s = 0; s < 8; s++) {
+  for (int s = 0; s < kNumStages; s++) {
     for (int k = 0; k < kStageSlots; k++) {
       if (c->ev.beg[s][k]) cudaEventDestroy(c->ev.beg[s][k]);
       if (c->ev.end[s][k]) cudaEventDestroy(c->ev.end[s][k]);
@@ -595,8 +595,8 @@ int tpm_ewald_fp64(tpm_ctx* c, int64_t ns, const int64_t* sample_idx, int method
 int tpm_get_stage_times(tpm_ctx* c, tpm_stage_times* out) {
   if (!c || !out) return fail(TPM_ERR_INVALID, "null argument");
   TPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  float t[8] = {0};
-  for (int s = 0; s < 8; s++) {
+  float t[kNumStages] = {0};
+  for (int s = 0; s < kNumStages; s++) {
     const int64_t n = std::min<int64_t>(c->ev.count[s], kStageSlots);
     double sum = 0;
     for (int64_t k = 0; k < n; k++) {
@@ -617,13 +617,14 @@ int tpm_get_stage_times(tpm_ctx* c, tpm_stage_times* out) {
   out->kick_ms = t[kStKick];
   out->drift_ms = t[kStDrift];
   out->ewald_ms = t[kStEwald];
+  out->interp_ms = t[kStInterp];
   return TPM_OK;
 }
 
 int tpm_reset_stage_times(tpm_ctx* c) {
   if (!c) return fail(TPM_ERR_INVALID, "null argument");
   TPM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  for (int s = 0; s < 8; s++) c->ev.count[s] = 0;
+  for (int s = 0; s < kNumStages; s++) c->ev.count[s] = 0;
   return TPM_OK;
 }
 

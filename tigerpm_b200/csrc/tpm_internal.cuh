@@ -47,13 +47,13 @@ struct TreeNode {
 // Per-stage CUDA event pairs, a ring of kStageSlots launches per stage, so
 // that the average over many steps can be read after they ran.
 constexpr int kStageSlots = 64;
+enum Stage { kStSort = 0, kStDeposit, kStFftF, kStGreen, kStFftI, kStKick, kStDrift, kStEwald, kStInterp,
+             kNumStages };
 struct StageEvents {
-  cudaEvent_t beg[8][kStageSlots];
-  cudaEvent_t end[8][kStageSlots];
-  int64_t count[8];   // records since the last reset
+  cudaEvent_t beg[kNumStages][kStageSlots];
+  cudaEvent_t end[kNumStages][kStageSlots];
+  int64_t count[kNumStages];  // records since the last reset
 };
-
-enum Stage { kStSort = 0, kStDeposit, kStFftF, kStGreen, kStFftI, kStKick, kStDrift, kStEwald };
 
 }  // namespace tpm
 
