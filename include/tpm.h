@@ -69,6 +69,13 @@ extern "C" {
  * (src/options.cpp:81-96).  The second block holds this library's extensions;
  * zero / negative values select the reference behaviour.
  */
+/* FFT of gravity_long_compute: the library's fused transforms (forward z
+ * and y, forward x + Green's function + inverse x in one pass, inverse y and
+ * z) when four_dim is a multiple of 16 of the form 2^a 3^b 5^c up to 1024,
+ * else cuFFT; or cuFFT always. */
+#define TPM_FFT_AUTO 0
+#define TPM_FFT_CUFFT 1
+
 typedef struct tpm_options {
   int four_dim;     /* PM grid points per side */
   int chain_dim;    /* chain-mesh cells per side */
@@ -94,6 +101,7 @@ typedef struct tpm_options {
   int kahan;           /* 1: compensated per-target PP sums (default 1) */
   int deterministic_deposit; /* 1: exact int64 fixed-point deposit, bit-reproducible;
                               * 0: FP32 shared-memory atomics (default, faster) */
+  int fft;             /* TPM_FFT_*: 3-D transforms of gravity_long_compute */
   uint64_t seed;       /* synthetic-input seed carried for drivers */
 } tpm_options;
 
@@ -145,7 +153,7 @@ int tpm_options_init(tpm_options* opts, int parts_dim, int parts_o_four, int fou
  * --four_o_chain, --box_size, --test, --config_file; src/options.cpp:47-55)
  * plus this library's extensions (--four_dim, --chain_dim, --rs_cells,
  * --rcut_over_rs, --assign=cloud4|cic|tsc, --sort=parity|fast, --kahan,
- * --hsoft, --seed) into opts.  Unknown flags are TPM_ERR_INVALID. */
+ * --hsoft, --seed, --fft=auto|cufft) into opts.  Unknown flags are TPM_ERR_INVALID. */
 int tpm_options_parse(tpm_options* opts, int argc, const char* const* argv);
 
 /* Creates a context for up to `capacity` particles on the current CUDA
@@ -277,6 +285,34 @@ int tpm_ctx_stream(tpm_ctx* ctx, void** stream);
  * sequence of the reference's kick_pme_test (src/test.cpp:182-234).  Kernel
  * error flags are collected on the device; read them with tpm_check_errors. */
 int tpm_pme_step(tpm_ctx* ctx, int min_rung, double scale, double t0, int first_call);
+
+/* Host arrays of one particle set (particles_X/U/R layout, n entries each).
+ * As an input, vx/vy/vz/rung may be NULL (zero); as an output, any NULL
+ * array is skipped. */
+typedef struct tpm_host_particles {
+  uint32_t* x;
+  uint32_t* y;
+  uint32_t* z;
+  float* vx;
+  float* vy;
+  float* vz;
+  int8_t* rung;
+} tpm_host_particles;
+
+/* A served stream of whole PME steps from and to host memory: for each s <
+ * nsteps, in[s] (n particles) is uploaded, chain-mesh sorted, given the PME
+ * long-range solve and kick_pme over the whole box, and the kicked particles
+ * (chain-mesh order, as tpm_get_particles returns them) are written to
+ * out[s].  Steps are independent boxes.  The upload of step s+1 and the
+ * download of step s-1 overlap step s's kernels (own copy streams; a third
+ * device particle set is allocated on the first call).  Host arrays should be
+ * page-locked for the overlap; pageable arrays work but serialise.  out[s]
+ * may repeat the same arrays (later steps overwrite earlier ones, in order).
+ * Returns when every output is written.  Replaces, per step, the reference's
+ * host staging and copy-back around kick_pme (src/kick_pme.cu:390-621). */
+int tpm_pme_steps_host(tpm_ctx* ctx, int64_t nsteps, int64_t n, const tpm_host_particles* in,
+                       const tpm_host_particles* out, int min_rung, double scale, double t0,
+                       int first_call);
 /* Synchronises and reports (then clears) device error flags raised since the
  * last check: TPM_ERR_RUNG for a clamped rung, TPM_ERR_INVALID for a drift
  * step beyond 2^31 box lengths. */

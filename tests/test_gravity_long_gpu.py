@@ -15,9 +15,9 @@ pytestmark = pytest.mark.gpu
 ASSIGN_ID = {"cloud4": 0, "cic": 1, "tsc": 2}
 
 
-def device_phi(ps, grid, assign, rs_cells, typ, chain=3, exact=False):
+def device_phi(ps, grid, assign, rs_cells, typ, chain=3, exact=False, fft="auto"):
     opts = make_options(round(ps.n ** (1 / 3)), grid, chain=chain, rs_cells=rs_cells, assign=assign,
-                        deterministic_deposit=exact)
+                        deterministic_deposit=exact, fft=fft)
     with TigerPM(opts, ps.n) as t:
         t.set_particles(ps)
         t.chainmesh_create()
@@ -104,3 +104,26 @@ def test_force_at():
         p, g = t.gravity_long_force_at(pos)
     rp, rg = force_at_numpy(full, pos)
     assert rel_rms(p, rp) < 1e-6 and rel_rms(g, rg) < 1e-6
+
+
+# The library's own transforms (fft3d.cu) run for grids that are multiples of
+# 16 made of the radices 16, 8, 4, 3, 5 and 2 (48 = 16.3, 80 = 16.5,
+# 96 = 16.3.2, 128 = 16.8, 160 = 16.5.2); each is compared against both the
+# oracle and cuFFT on the same deposit.
+@pytest.mark.parametrize("grid", [48, 80, 96, 128, 160])
+def test_library_fft_matches_oracle_and_cufft(grid):
+    ps = particle_set("uniform", 20, 4)
+    for typ in (GRAVITY_LONG_PME, GRAVITY_LONG_PM):
+        phi, (x, y, z) = device_phi(ps, grid, "cloud4", 2.0, typ, exact=True)
+        phi_cu, _ = device_phi(ps, grid, "cloud4", 2.0, typ, exact=True, fft="cufft")
+        ref = O.gravity_long(grid, 2.0, 0, x, y, z, pme=typ)
+        assert rel_rms(phi, ref) < 2e-6, (grid, typ, rel_rms(phi, ref))
+        assert rel_rms(phi, phi_cu) < 2e-6, (grid, typ, rel_rms(phi, phi_cu))
+
+
+def test_library_fft_768_matches_cufft():
+    """The benchmark mesh (768 = 4^4 x 3) against cuFFT on one deposit."""
+    ps = particle_set("uniform", 64, 5)
+    phi, _ = device_phi(ps, 768, "cloud4", 2.0, GRAVITY_LONG_PME, chain=64, exact=True)
+    phi_cu, _ = device_phi(ps, 768, "cloud4", 2.0, GRAVITY_LONG_PME, chain=64, exact=True, fft="cufft")
+    assert rel_rms(phi, phi_cu) < 2e-6, rel_rms(phi, phi_cu)

@@ -29,6 +29,7 @@ GRAVITY_LONG_PM = 0
 GRAVITY_LONG_PME = 1
 ASSIGN = {"cloud4": 0, "cic": 1, "tsc": 2}
 SORT = {"parity": 0, "fast": 1}
+FFT = {"auto": 0, "cufft": 1}
 
 
 class Options(C.Structure):
@@ -43,7 +44,7 @@ class Options(C.Structure):
         ("z0", C.c_double),
         ("rcut_over_rs", C.c_double), ("assign", C.c_int), ("deconv_order", C.c_int),
         ("sort_mode", C.c_int), ("kahan", C.c_int), ("deterministic_deposit", C.c_int),
-        ("seed", C.c_uint64),
+        ("fft", C.c_int), ("seed", C.c_uint64),
     ]
 
 
@@ -51,6 +52,11 @@ class StageTimes(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("sort_ms", "deposit_ms", "fft_forward_ms", "green_ms",
                                          "fft_inverse_ms", "kick_ms", "drift_ms", "ewald_ms",
                                          "interp_ms")]
+
+
+class HostParticles(C.Structure):
+    """struct tpm_host_particles: host array addresses of one particle set."""
+    _fields_ = [(n, C.c_void_p) for n in ("x", "y", "z", "vx", "vy", "vz", "rung")]
 
 
 class DeviceArrays(C.Structure):
@@ -101,6 +107,7 @@ SIGNATURES = [
     ("tpm_synchronize", _I, [_P]),
     ("tpm_ctx_stream", _I, [_P, C.POINTER(_P)]),
     ("tpm_pme_step", _I, [_P, _I, _D, _D, _I]),
+    ("tpm_pme_steps_host", _I, [_P, _I64, _I64, _P, _P, _I, _D, _D, _I]),
     ("tpm_check_errors", _I, [_P]),
     ("tpm_count_pairs", _I, [_P, _I, C.POINTER(_I64), C.POINTER(_I64)]),
     ("tpm_fp32_peak_probe", _I, [C.POINTER(_D)]),

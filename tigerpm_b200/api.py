@@ -75,7 +75,8 @@ def process_options(argv) -> Options:
 
 def make_options(n_side: int, grid: int, chain: int | None = None, rs_cells: float = 1.0,
                  rcut_over_rs: float = 0.0, assign: str = "cloud4", sort: str = "parity",
-                 kahan: bool = True, GM: float = 1.0, deterministic_deposit: bool = False) -> Options:
+                 kahan: bool = True, GM: float = 1.0, deterministic_deposit: bool = False,
+                 fft: str = "auto") -> Options:
     """Options for a box of n_side^3 particles on a grid^3 mesh.  chain=None
     picks the largest chain mesh whose cells are at least the cutoff wide
     (or rcut = 4.5 rs wide when there is no cutoff)."""
@@ -92,6 +93,7 @@ def make_options(n_side: int, grid: int, chain: int | None = None, rs_cells: flo
     o.sort_mode = _lib.SORT[sort]
     o.kahan = 1 if kahan else 0
     o.deterministic_deposit = 1 if deterministic_deposit else 0
+    o.fft = _lib.FFT[fft]
     o.GM = GM
     return o
 
@@ -328,6 +330,26 @@ class TigerPM:
         """chainmesh_create + gravity_long_compute(PME) + kick_pme, no host sync."""
         check(self.lib.tpm_pme_step(self.h, int(min_rung), float(scale), float(t0), 1 if first_call else 0),
               "pme_step")
+
+    def pme_steps_host(self, inputs, outputs, min_rung: int = 0, scale: float = 1.0, t0: float = 1.0,
+                       first_call: bool = True) -> None:
+        """Served stream: one whole PME step per input particle set, host to
+        host, transfers overlapped with the neighbouring steps' kernels.
+        inputs / outputs: sequences of objects with x, y, z, vx, vy, vz, rung
+        arrays (outputs may repeat one set).  Arrays must be C-contiguous and
+        stay alive for the call."""
+        ns = len(inputs)
+        if len(outputs) != ns:
+            raise ValueError("one output set per input set")
+        n = int(inputs[0].x.size) if ns else 0
+        def hp(p):
+            return _lib.HostParticles(*[a.ctypes.data if hasattr(a, "ctypes") else int(a) for a in
+                                        (p.x, p.y, p.z, p.vx, p.vy, p.vz, p.rung)])
+        ins = (_lib.HostParticles * max(ns, 1))(*[hp(p) for p in inputs])
+        outs = (_lib.HostParticles * max(ns, 1))(*[hp(p) for p in outputs])
+        check(self.lib.tpm_pme_steps_host(self.h, ns, n, ins, outs, int(min_rung), float(scale), float(t0),
+                                          1 if first_call else 0), "pme_steps_host")
+        self.n = n
 
     def check_errors(self) -> None:
         check(self.lib.tpm_check_errors(self.h), "check_errors")

@@ -311,6 +311,8 @@ int mesh_init(tpm_ctx* c) {
   TPM_CUDA_TRY(cudaMemcpy(c->gtab, g.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
   TPM_CUDA_TRY(cudaMemcpy(c->gtab + N, g_pm.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
   TPM_CUDA_TRY(cudaMemcpy(c->k2tab, k2.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+  c->use_fft3d = c->opt.fft != TPM_FFT_CUFFT && fft3d_supported(N);
+  if (c->use_fft3d) return fft3d_init(c);
   TPM_CUFFT_TRY(cufftPlan3d(&c->plan_r2c, N, N, N, CUFFT_R2C));
   TPM_CUFFT_TRY(cufftPlan3d(&c->plan_c2r, N, N, N, CUFFT_C2R));
   TPM_CUFFT_TRY(cufftSetStream(c->plan_r2c, c->stream));
@@ -345,6 +347,12 @@ int gravity_long(tpm_ctx* c, int type) {
   }
   if (rc) return rc;
   stage_end(c, kStDeposit);
+  if (c->use_fft3d) {
+    rc = fft3d_poisson(c, type == TPM_GRAVITY_LONG_PME ? c->gtab : c->gtab + N);
+    if (rc) return rc;
+    c->have_phi = true;
+    return TPM_OK;
+  }
   stage_begin(c, kStFftF);
   TPM_CUFFT_TRY(cufftExecR2C(c->plan_r2c, c->rho, c->rhok));
   stage_end(c, kStFftF);

@@ -62,7 +62,7 @@ int64_t plan_bytes(const tpm_options& o, int64_t cap) {
   b += 4 * (2 * ((cap + 4095) / 4096 + (ncell + 4095) / 4096) + 64);  // blocksums
   b += 8 * ((std::max(cap, ncell) + 4095) / 4096 + 1);  // look-back status words
   b += 8 * (ncell + 2);                        // counts + offsets
-  b += N * N * N * 4 * 2 + N * N * (N / 2 + 1) * 8;  // rho, phi, rhok
+  b += N * N * N * 4 * 2 + N * N * (int64_t)fft3d_padded_columns((int)N) * 8 + N * 8;  // rho, phi, rhok, twiddles
   return b;
 }
 
@@ -74,6 +74,7 @@ int derive(tpm_ctx* c) {
   if (!(o.rs > 0) || !(o.hsoft > 0)) return fail(TPM_ERR_INVALID, "rs and hsoft must be positive");
   if (o.assign < 0 || o.assign > 2) return fail(TPM_ERR_INVALID, "assign must be cloud4, cic or tsc");
   if (o.sort_mode < 0 || o.sort_mode > 1) return fail(TPM_ERR_INVALID, "sort_mode must be parity or fast");
+  if (o.fft < 0 || o.fft > 1) return fail(TPM_ERR_INVALID, "fft must be auto or cufft");
   c->N = o.four_dim;
   c->C = o.chain_dim;
   c->rs_box = o.rs;
@@ -158,7 +159,7 @@ int tpm_options_init(tpm_options* o, int parts_dim, int parts_o_four, int four_o
 int tpm_options_parse(tpm_options* o, int argc, const char* const* argv) {
   if (!o) return fail(TPM_ERR_INVALID, "null options");
   int parts_dim = 130, parts_o_four = 3, four_o_chain = 5;  // src/options.cpp:50-52 defaults
-  int four_dim = 0, chain_dim = 0, kahan = 1, sort_mode = 0, assign = 0, det_dep = 0;
+  int four_dim = 0, chain_dim = 0, kahan = 1, sort_mode = 0, assign = 0, det_dep = 0, fft = TPM_FFT_AUTO;
   double rs_cells = 0, rcut = 0, hsoft = 0, box_size = 1;
   unsigned long long seed = 1;
   for (int i = 0; i < argc; i++) {
@@ -193,6 +194,10 @@ int tpm_options_parse(tpm_options* o, int argc, const char* const* argv) {
       if (val == "parity") sort_mode = 0;
       else if (val == "fast") sort_mode = 1;
       else ok = false;
+    } else if (key == "fft") {
+      if (val == "auto") fft = TPM_FFT_AUTO;
+      else if (val == "cufft") fft = TPM_FFT_CUFFT;
+      else ok = false;
     } else return fail(TPM_ERR_INVALID, "unknown option --" + key);
     if (!ok) return fail(TPM_ERR_INVALID, "bad value for --" + key + ": " + val);
   }
@@ -218,6 +223,7 @@ int tpm_options_parse(tpm_options* o, int argc, const char* const* argv) {
   o->rcut_over_rs = rcut;
   o->assign = assign;
   o->sort_mode = sort_mode;
+  o->fft = fft;
   o->kahan = kahan;
   o->deterministic_deposit = det_dep;
   o->seed = seed;
@@ -290,7 +296,8 @@ int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out) {
   A.get(c->tree, C * kMaxTreeDepth);
   A.get(c->depth1d, C);
   A.get(c->rho, N * N * N);
-  A.get(c->rhok, N * N * (N / 2 + 1));
+  A.get(c->rhok, N * N * fft3d_padded_columns((int)N));
+  A.get(c->fft_tw, N);
   A.get(c->phi, N * N * N);
   A.get(c->gtab, 2 * N);
   A.get(c->k2tab, N);
@@ -322,7 +329,7 @@ int tpm_ctx_destroy(tpm_ctx* c) {
   void* ptrs[] = {c->x, c->y, c->z, c->vx, c->vy, c->vz, c->rung, c->gx, c->gy, c->gz, c->pot, c->pos4,
                   c->x2, c->y2, c->z2, c->vx2, c->vy2, c->vz2, c->rung2, c->key, c->idx, c->cellof,
                   c->prefix, c->slot, c->blocksum, c->scan_status, c->cell_count, c->cell_begin, c->thr, c->tree,
-                  c->depth1d, c->rho, c->rhok, c->phi, c->gtab, c->k2tab, c->d_err};
+                  c->depth1d, c->rho, c->rhok, c->fft_tw, c->phi, c->gtab, c->k2tab, c->d_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->plans) {
@@ -335,6 +342,7 @@ int tpm_ctx_destroy(tpm_ctx* c) {
       if (c->ev.end[s][k]) cudaEventDestroy(c->ev.end[s][k]);
     }
   }
+  stream_destroy(c);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return TPM_OK;

@@ -99,7 +99,9 @@ struct tpm_ctx {
 
   // mesh
   float* rho = nullptr;  // N^3 real grid (deposit out, r2c in)
-  cufftComplex* rhok = nullptr;
+  cufftComplex* rhok = nullptr;  // N x N x Sz spectrum (Sz = N/2+1 rounded up to 8)
+  float2* fft_tw = nullptr;       // exp(-2 pi i m / N), m < N, for the library's own transforms
+  bool use_fft3d = false;         // library transforms instead of cuFFT
   float* phi = nullptr;  // N^3
   float* gtab = nullptr;   // exp(-k^2 rs^2) sinc(k/2)^-p per index, N
   float* k2tab = nullptr;  // k^2 per index, N
@@ -109,6 +111,14 @@ struct tpm_ctx {
   // ewald scratch
   double* ew_buf = nullptr;
   int64_t ew_cap = 0;
+
+  // served stream (stream.cu): a third particle set, copy streams and event rings
+  uint32_t *x3 = nullptr, *y3 = nullptr, *z3 = nullptr;
+  float *vx3 = nullptr, *vy3 = nullptr, *vz3 = nullptr;
+  int8_t* rung3 = nullptr;
+  cudaStream_t up_stream = nullptr, down_stream = nullptr;
+  cudaEvent_t ev_up[3] = {}, ev_done[3] = {}, ev_down[3] = {};
+  bool pipe_ready = false;
 
   int* d_err = nullptr;
   int64_t launches = 0;
@@ -134,6 +144,11 @@ int drift(tpm_ctx* c, double dt);
 int ewald(tpm_ctx* c, int64_t ns, const uint32_t* dsx, const uint32_t* dsy, const uint32_t* dsz,
           int method, double* phi, double* gx, double* gy, double* gz);
 int mesh_init(tpm_ctx* c);
+int fft3d_padded_columns(int N);
+bool fft3d_supported(int N);
+int fft3d_init(tpm_ctx* c);
+int fft3d_poisson(tpm_ctx* c, const float* gt);
+void stream_destroy(tpm_ctx* c);
 int sort_init(tpm_ctx* c);
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
