@@ -18,9 +18,10 @@
 //       two rows of phi
 //
 // The spectrum lives in a [N][N][Sz] complex array, Sz = N/2+1 rounded up to
-// 8 so that a block's 8 kz columns start on a 64-byte boundary (the padding
-// columns are zero and never reach phi).  Each block holds 8 lines of length
-// N in shared memory and transforms them with a self-sorting (Stockham)
+// the lines per block (4) so that a block's kz columns start on a 32-byte
+// boundary (the padding columns are zero and never reach phi).  Each block
+// holds 4 lines of length N in shared memory and transforms them with a
+// self-sorting (Stockham)
 // radix-16/8/4/3/5/2 FFT, each stage from one shared buffer into the other.  Twiddles
 // exp(-2 pi i m / N) are computed in FP64 on the host and staged in shared
 // memory.  Forward transforms use exp(-i...), inverse exp(+i...), both
@@ -148,11 +149,11 @@ struct Dft<8, S> : DftSplit<8, S> {};
 template <int S>
 struct Dft<16, S> : DftSplit<16, S> {};
 
-// One Stockham stage of radix R over the 8 lines of length N (line stride
-// LS), from shared buffer x to shared buffer y: butterfly j of a line reads
-// x[j + r N/R], applies the twiddles exp(S 2 pi i (j mod Ns) r / (Ns R)),
+// One Stockham stage of radix R over the block's lines of length N (line
+// stride LS), from shared buffer x to shared buffer y: butterfly j of a line
+// reads x[j + r N/R], applies the twiddles exp(S 2 pi i (j mod Ns) r / (Ns R)),
 // and writes y[(j / Ns) Ns R + (j mod Ns) + r Ns].  Thread t takes line
-// t mod 8 and butterflies j = t / 8 + 64 i; j / Ns is a multiply-high by
+// t mod L and butterflies j = t / L + 64 i; j / Ns is a multiply-high by
 // ceil(2^32 / Ns), exact while j Ns < 2^32.
 template <int R, int S>
 __device__ __forceinline__ void fft_stage(const float2* __restrict__ x, float2* __restrict__ y,
@@ -192,7 +193,7 @@ struct FftPlan {
   unsigned ns_inv[12];  // ceil(2^32 / Ns) of each stage
 };
 
-// Full transform of the 8 lines (S = -1 forward, +1 inverse) that start in
+// Full transform of the block's lines (S = -1 forward, +1 inverse) that start in
 // a; b is the second buffer.  Returns the buffer holding the result.
 template <int S>
 __device__ __forceinline__ float2* block_fft(float2* a, float2* b, const float2* __restrict__ tw, const FftPlan& p,
@@ -215,9 +216,9 @@ __device__ __forceinline__ float2* block_fft(float2* a, float2* b, const float2*
   return a;
 }
 
-// Line stride in shared memory: N + 2 complex values.  Accesses where the
-// eight lines of a warp run fastest (8 lines x 2 positions per half-warp) then
-// fall in 16 distinct bank pairs.
+// Line stride in shared memory: N + 16/L complex values.  With the lines of
+// a warp running fastest (L lines x 16/L positions per half-warp), the
+// half-warp's 16 accesses then fall in 16 distinct bank pairs.
 __device__ __forceinline__ int line_stride(int N) { return N + 16 / kFftLines; }
 
 __device__ __forceinline__ void load_twiddles(float2* s_tw, const float2* __restrict__ tw, int N) {
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_z_r2c(const float* __restri
   }
 }
 
-// P2 / P4: transform along y of the 8 kz columns [c0, c0 + 8) of plane x.
+// P2 / P4: transform along y of the L kz columns [c0, c0 + L) of plane x.
 template <int S>
 __global__ void __launch_bounds__(kFftThreads) k_fft_y(float2* __restrict__ Y, FftPlan p,
                                                        const float2* __restrict__ tw) {
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_y(float2* __restrict__ Y, F
   }
 }
 
-// P3: forward transform along x of the 8 kz columns [c0, c0 + 8) of row y,
+// P3: forward transform along x of the L kz columns [c0, c0 + L) of row y,
 // the Green's function (apply_laplacian, src/gravity_long.cpp:214-239; the
 // same separable tables and FP32 expression as the cuFFT path's k_green),
 // and the inverse transform along x.
