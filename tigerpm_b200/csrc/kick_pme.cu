@@ -73,6 +73,7 @@ struct KickArgs {
   int kahan;
   float GM, eta, t0, scale, hsoft;
   float inv2rs, twooversqrtpi, h2, hinv, h3inv, rcut2;
+  float p_r, e_r, c_r;  // A&S p, -log2(e), 2/sqrt(pi), each times powers of 1/(2 r_s)
 };
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
@@ -292,29 +293,32 @@ __device__ __forceinline__ void pair(const KickArgs& a, float dx, float dy, floa
     dz -= rintf(dz);
   }
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float r2c = fmaxf(r2, a.h2);
+  // Pairs beyond the cutoff take r^2 = 1e30: 1/r, erfc and exp(-x^2) then
+  // vanish and the pair adds exactly 0, without a mask on the results.
+  const float r2c = r2 < a.rcut2 ? fmaxf(r2, a.h2) : 1e30f;
   const float rinv = rsqrt_approx(r2c);
-  const float x0 = r2c * rinv * a.inv2rs;
-  const float t = rcp_approx(fmaf(0.3275911f, x0, 1.0f));
-  const float e = ex2_approx(-1.4426950408889634f * x0 * x0);
+  const float r = r2c * rinv;
+  // x0 = r / (2 r_s); the constants carry 1/(2 r_s): p x0 = p_r r,
+  // -log2(e) x0^2 = e_r r^2, (2/sqrt(pi)) x0 = c_r r
+  const float t = rcp_approx(fmaf(a.p_r, r, 1.0f));
+  const float e = ex2_approx(a.e_r * r2c);
   const float poly =
       t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f), 0.254829592f);
   const float erfc0 = poly * e;
   const float rinv2 = rinv * rinv;
-  float rinv3 = fmaf(a.twooversqrtpi * x0, e, erfc0) * rinv2 * rinv;
-  float rinv1 = erfc0 * rinv;
+  float rinv3 = fmaf(a.c_r * r, e, erfc0) * rinv2 * rinv;
+  float rinv1 = erfc0;  // times 1/r below
+  float rscale = rinv;
   if (r2 <= a.h2) {  // softened Newtonian kernel inside hsoft (rare)
     const float q2 = r2 * a.hinv * a.hinv;
     rinv3 = fmaf(fmaf(15.0f / 8.0f, q2, -21.0f / 4.0f), q2, 35.0f / 8.0f) * a.h3inv;
-    rinv1 = fmaf(fmaf(fmaf(-5.0f / 16.0f, q2, 21.0f / 16.0f), q2, -35.0f / 16.0f), q2, 35.0f / 16.0f) * a.hinv;
+    rinv1 = fmaf(fmaf(fmaf(-5.0f / 16.0f, q2, 21.0f / 16.0f), q2, -35.0f / 16.0f), q2, 35.0f / 16.0f);
+    rscale = a.hinv;
   }
-  const bool in = r2 < a.rcut2;
-  rinv3 = in ? rinv3 : 0.0f;
-  rinv1 = in ? rinv1 : 0.0f;
   gx = fmaf(-dx, rinv3, gx);
   gy = fmaf(-dy, rinv3, gy);
   gz = fmaf(-dz, rinv3, gz);
-  ph -= rinv1;
+  ph = fmaf(-rinv1, rscale, ph);
 }
 
 
@@ -638,6 +642,9 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
   const float rs = (float)c->rs_box;
   a.inv2rs = 1.0f / rs / 2.0f;
   a.twooversqrtpi = 2.0f / sqrtf((float)M_PI);
+  a.p_r = 0.3275911f * a.inv2rs;
+  a.e_r = -1.4426950408889634f * a.inv2rs * a.inv2rs;
+  a.c_r = a.twooversqrtpi * a.inv2rs;
   a.h2 = a.hsoft * a.hsoft;
   a.hinv = 1.f / a.hsoft;
   a.h3inv = a.hinv * (a.hinv * a.hinv);
