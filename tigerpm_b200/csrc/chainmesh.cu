@@ -274,8 +274,9 @@ __device__ __forceinline__ unsigned long long pack_status(unsigned stamp, unsign
 // One partition level, part 1: the left-child flags of every position and
 // their exclusive prefix, in a single pass (chained scan with decoupled
 // look-back; tiles are taken in launch order through an atomic counter, so
-// every predecessor a tile waits on is already running).  The look-back spin
-// is bounded: on expiry the tile records kErrTimeout and uses 0.
+// every predecessor a tile waits on is already running).  The look-back is
+// done by one warp, 32 predecessor tiles at a time; its spin is bounded: on
+// expiry the tile records kErrTimeout and uses what it has summed.
 __global__ void __launch_bounds__(kScanThreads) k_level_scan(LevelArgs a, unsigned stamp, int* __restrict__ counter,
                                                              unsigned long long* __restrict__ status,
                                                              int32_t* __restrict__ prefix, int* __restrict__ err) {
@@ -298,33 +299,47 @@ __global__ void __launch_bounds__(kScanThreads) k_level_scan(LevelArgs a, unsign
     s += v[k];
   }
   const int off = block_exclusive_scan(s, warp_tot, &total);
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
+    // warp-parallel look-back: lane l reads the status of tile (top - l);
+    // once all 32 are published, the aggregates up to the closest inclusive
+    // prefix are summed, else the window moves 32 tiles back
+    const int lane = threadIdx.x;
     const int agg = total;
     int excl = 0;
     if (tile == 0) {
-      atomicExch(status, pack_status(stamp, kFlagIncl, agg));
+      if (lane == 0) atomicExch(status, pack_status(stamp, kFlagIncl, agg));
     } else {
-      atomicExch(status + tile, pack_status(stamp, kFlagAgg, agg));
-      int j = tile - 1;
+      if (lane == 0) atomicExch(status + tile, pack_status(stamp, kFlagAgg, agg));
+      int top = tile - 1;
       long long spins = 0;
-      while (j >= 0) {
-        const unsigned long long w = *reinterpret_cast<volatile unsigned long long*>(status + j);
-        const unsigned wstamp = (unsigned)(w >> 34);
-        const unsigned long long f = (w >> 32) & 3ull;
-        if (wstamp != stamp || f == 0) {
-          if (++spins > (1ll << 24)) {
-            atomicOr(err, kErrTimeout);
+      while (true) {
+        const int j = top - lane;
+        unsigned long long f = kFlagIncl;  // before tile 0: an inclusive zero
+        int v = 0;
+        if (j >= 0) {
+          const unsigned long long w = *reinterpret_cast<volatile unsigned long long*>(status + j);
+          f = (unsigned)(w >> 34) == stamp ? (w >> 32) & 3ull : 0ull;
+          v = (int)(unsigned)(w & 0xffffffffull);
+        }
+        if (__any_sync(0xffffffffu, f == 0)) {
+          if (++spins > (1ll << 22)) {
+            if (lane == 0) atomicOr(err, kErrTimeout);
             break;
           }
           continue;
         }
-        excl += (int)(unsigned)(w & 0xffffffffull);
-        if (f == kFlagIncl) break;
-        j--;
+        const unsigned incl = __ballot_sync(0xffffffffu, f == kFlagIncl);
+        const int first = incl ? __ffs(incl) - 1 : 32;
+        int sum = lane <= first ? v : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        excl += sum;
+        if (incl) break;
+        top -= 32;
       }
-      atomicExch(status + tile, pack_status(stamp, kFlagIncl, excl + agg));
+      if (lane == 0) atomicExch(status + tile, pack_status(stamp, kFlagIncl, excl + agg));
     }
-    excl_s = excl;
+    if (lane == 0) excl_s = excl;
   }
   __syncthreads();
   int run = excl_s + off;
