@@ -413,10 +413,12 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
   __syncthreads();
   const int total = runp[kMaxRuns];
   float4* buf = bufs + warp * kBuf;
-  for (int32_t sbase = pb; sbase < pe; sbase += npass) {
+  int np = 8;  // sinks per pass: the power of two >= the cell's count, at most npass
+  while (np < npass && np < pe - pb) np <<= 1;
+  for (int32_t sbase = pb; sbase < pe; sbase += np) {
     // 1. order this pass's active sinks by sub-cell (deterministic bitonic sort)
-    if (tid == 0) runp[kMaxRuns + 1] = npass;  // active count when every slot is active
-    for (int e = tid; e < npass; e += T) {
+    if (tid == 0) runp[kMaxRuns + 1] = np;  // active count when every slot is active
+    for (int e = tid; e < np; e += T) {
       const int32_t i = sbase + e;
       unsigned k = 512u;  // inactive / absent sinks sort last
       if (i < pe && a.rung[i] >= a.min_rung) {
@@ -426,9 +428,9 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
       skey[e] = (k << 8) | (unsigned)e;
     }
     __syncthreads();
-    for (int kk = 2; kk <= npass; kk <<= 1) {
+    for (int kk = 2; kk <= np; kk <<= 1) {
       for (int j = kk >> 1; j > 0; j >>= 1) {
-        for (int e = tid; e < npass; e += T) {
+        for (int e = tid; e < np; e += T) {
           const int ixj = e ^ j;
           if (ixj > e) {
             const unsigned u = skey[e], v = skey[ixj];
@@ -442,7 +444,7 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
         __syncthreads();
       }
     }
-    for (int e = tid; e < npass; e += T) {
+    for (int e = tid; e < np; e += T) {
       const unsigned m = skey[e];
       const bool act = (m >> 8) < 512u;
       float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
