@@ -63,6 +63,21 @@ FLOPS_PER_PAIR = 44.0      # in-cutoff pair, FMA = 2, MUFU = 1 (the reference's 
 FLOPS_PER_CULLED = 8.0     # candidate pair rejected by the r^2 test
 
 
+def max_over_ranks(ms, dist, device=None):
+    """Largest per-rank time (every rank calls it; dist None: one process)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(n_per_rank, world, steps, ms):
+    """Whole-job particle-kicks/s: every rank's particles over the slowest rank's time."""
+    return n_per_rank * world * steps / (ms * 1e-3)
+
+
 def make_particles(cfg, seed):
     from tigerpm_b200 import workloads as W
     if cfg["kind"] == "uniform":
@@ -202,12 +217,7 @@ def gpu_arm(args, cfg, name, rank, world, dist):
             fn()
         e1.record(ext)
         e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(e0.elapsed_time(e1), dist, dev)
 
     for _ in range(args.warmup):
         step_resident()
@@ -234,16 +244,12 @@ def gpu_arm(args, cfg, name, rank, world, dist):
     barrier()
     t_host = time.perf_counter()
     ctx.pme_steps_host([host_in] * args.steps, [host_out] * args.steps)
-    ms_e2e = (time.perf_counter() - t_host) * 1e3
-    if dist is not None:
-        t = torch.tensor([ms_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks((time.perf_counter() - t_host) * 1e3, dist, dev)
 
     total = n * world * args.steps
     out = {
-        "value": total / (ms * 1e-3), "ms_per_step": ms / args.steps,
-        "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "particle-kicks/s",
+        "value": replica_rate(n, world, args.steps, ms), "ms_per_step": ms / args.steps,
+        "e2e": {"value": replica_rate(n, world, args.steps, ms_e2e), "unit": "particle-kicks/s",
                 "h2d_bytes_per_step": int(sum(t.numel() * t.element_size() for t in pinned_in)),
                 "d2h_bytes_per_step": int(sum(t.numel() * t.element_size() for t in pinned_out)),
                 "ms_per_step": ms_e2e / args.steps, "api": "tpm_pme_steps_host (served stream)",
