@@ -61,6 +61,21 @@ __device__ __forceinline__ int stencil(uint32_t raw, int N, float* w) {
   }
 }
 
+// Offset of the first stencil point from floor(X N) before the TSC
+// rounding: cloud4 starts at I - 1, CIC at I, TSC at I - 1 or I (taken as
+// I - 1 with one extra point of reach in touches()).
+template <int ASSIGN>
+constexpr int kStencilOff = ASSIGN == TPM_ASSIGN_CIC ? 0 : -1;
+
+// Does a run of W (+1 for TSC's rounding) points starting at d (relative to
+// the tile origin, any integer) meet [0, ext) on a periodic axis of N?
+template <int W>
+__device__ __forceinline__ bool touches(int d, int N, int ext) {
+  if (d < 0) d += N;  // d = stencil start (-1 .. N+1) minus a tile origin in [0, N)
+  if (d >= N) d -= N;
+  return d < ext || d + W + 1 > N;
+}
+
 template <int ASSIGN>
 struct Width {
   static constexpr int W = ASSIGN == TPM_ASSIGN_CLOUD4 ? 4 : (ASSIGN == TPM_ASSIGN_CIC ? 2 : 3);
@@ -143,6 +158,15 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
         const int32_t pb = __ldg(a.begin + row + ca), pe = __ldg(a.begin + row + cb);
         for (int32_t p = pb + threadIdx.x; p < pe; p += blockDim.x) {
           const int4 q = __ldg(a.pos4 + p);
+          // first stencil point per dim relative to the tile, wrapped into
+          // [-N/2, N/2): the particle touches the tile only if every dim's
+          // W points meet [0, ext)
+          const int s0 = (int)(((uint64_t)(uint32_t)q.x * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
+          const int s1 = (int)(((uint64_t)(uint32_t)q.y * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
+          const int s2 = (int)(((uint64_t)(uint32_t)q.z * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
+          if (!touches<W>(s0 - o[0], N, ext[0]) || !touches<W>(s1 - o[1], N, ext[1]) ||
+              !touches<W>(s2 - o[2], N, ext[2]))
+            continue;
           float wx[4], wy[4], wz[4];
           int r[3];
           r[0] = stencil<ASSIGN>((uint32_t)q.x, N, wx) - o[0];
