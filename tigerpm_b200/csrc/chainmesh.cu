@@ -34,6 +34,7 @@ namespace {
 constexpr int kScanThreads = 512;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
+static_assert(kScanTile == kScanTileElems, "scan tiles must match the status and block-sum arrays");
 
 // Cell coordinate of raw position r along one axis: the largest m with
 // r >= thr[m] (thr[0] = 0).  The integer estimate floor(r*C/2^32) is within

@@ -59,8 +59,9 @@ int64_t plan_bytes(const tpm_options& o, int64_t cap) {
   b += cap * (3 * 4 + 3 * 4 + 1);              // permutation targets
   b += cap * 16;                               // pos4
   b += cap * 4 * 5 + 8;                        // key, idx, cellof, prefix, slot
-  b += 4 * (2 * ((cap + 4095) / 4096 + (ncell + 4095) / 4096) + 64);  // blocksums
-  b += 8 * ((std::max(cap, ncell) + 4095) / 4096 + 1);  // look-back status words
+  const int64_t T = kScanTileElems;
+  b += 4 * (2 * ((cap + T - 1) / T + (ncell + T - 1) / T) + 64);  // blocksums
+  b += 8 * ((std::max(cap, ncell) + T - 1) / T + 1);  // look-back status words
   b += 8 * (ncell + 2);                        // counts + offsets
   b += N * N * N * 4 * 2 + N * N * (int64_t)fft3d_padded_columns((int)N) * 8 + N * 8;  // rho, phi, rhok, twiddles
   return b;
@@ -262,7 +263,7 @@ int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out) {
   }
   c->cap = capacity;
   const int64_t N = c->N, C = c->C, ncell = C * C * C;
-  const int64_t nb = (std::max(capacity, ncell) + 4095) / 4096;
+  const int64_t nb = (std::max(capacity, ncell) + kScanTileElems - 1) / kScanTileElems;
   Alloc A{c};
   A.get(c->x, capacity);
   A.get(c->y, capacity);

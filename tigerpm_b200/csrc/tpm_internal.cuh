@@ -15,6 +15,10 @@ namespace tpm {
 constexpr int kMaxRung = 32;      // MAX_RUNG, tigerpm/tigerpm.hpp:34
 constexpr int kNInterp = 6;       // NINTERP, tigerpm/tigerpm.hpp:35
 constexpr int kPhiBW = 3;         // PHI_BW, tigerpm/tigerpm.hpp:41
+// Elements per tile of the sort's scans: sizes the per-tile block sums and
+// look-back status words allocated with the context (chainmesh.cu checks
+// that its scan kernels use the same tile).
+constexpr int kScanTileElems = 4096;
 constexpr int kMaxTreeDepth = 24; // 1-D bisection depth bound (C < 2^23)
 constexpr int kDepositFracBits = 40;
 
