@@ -61,6 +61,7 @@ CONFIGS = {
 METRIC = "PME particle-kicks/s at rms force err<=1e-4 vs FP64 Ewald"
 FLOPS_PER_PAIR = 44.0      # in-cutoff pair, FMA = 2, MUFU = 1 (the reference's inner loop)
 FLOPS_PER_CULLED = 8.0     # candidate pair rejected by the r^2 test
+REF_BUDGET_S = 150.0       # CPU seconds the reference arm spends on timed whole kicks
 
 
 def max_over_ranks(ms, dist, device=None):
@@ -109,7 +110,9 @@ def workload_desc(name, cfg, opts):
         "particles": cfg["n_side"] ** 3, "grid": cfg["grid"], "assign": cfg["assign"], "rs_cells": cfg["rs_cells"],
         "rcut_over_rs": cfg["rcut_over_rs"], "chain_dim": opts.chain_dim, "sort": "parity",
         "precision": "fp32 pair terms, Kahan-compensated per-target sums",
-        "l2": "inputs larger than L2 (particles + mesh > 126 MB)",
+        "l2": ("inputs larger than L2 (particles + mesh > 126 MB)"
+               if 25 * cfg["n_side"] ** 3 + 12 * cfg["grid"] ** 3 > 126e6 else
+               "inputs smaller than L2; no flush (secondary, launch-bound entry)"),
     }
 
 
@@ -280,6 +283,99 @@ def gpu_arm(args, cfg, name, rank, world, dist):
     return out
 
 
+def ensemble_opts(sides):
+    from tigerpm_b200 import workloads as W
+    from tigerpm_b200.api import make_options
+    out = []
+    for n in sides:
+        p = W.accurate_box_params(int(n))
+        out.append(make_options(p["n_side"], p["grid"], rs_cells=p["rs_cells"], rcut_over_rs=p["rcut_over_rs"],
+                                assign=p["assign"]))
+    return out
+
+
+def ensemble_accuracy(boxes, sets, samples_per_box, seed):
+    """Vector rms force error over a few boxes of an ensemble, each against
+    its own FP64 Ewald sum, pooled as one sum of squares."""
+    from tigerpm_b200 import workloads as W
+    num = den = 0.0
+    count = 0
+    for j, t in boxes:
+        idx = W.sample_indices(sets[j].n, samples_per_box, seed + j)
+        gx, gy, gz, _ = t.get_forces()
+        _, g = t.ewald_samples(idx, 1)
+        gk = np.stack([gx[idx], gy[idx], gz[idx]], axis=1).astype(np.float64)
+        num += float(np.sum((gk - g) ** 2))
+        den += float(np.sum(g * g))
+        count += idx.size
+    return {"force_rms_vector": float(f"{math.sqrt(num / den):.4e}"), "samples": count, "boxes": len(boxes)}
+
+
+def batch_arm(args, rank, world, dist, n_boxes=64, lo=32, hi=128):
+    """Config 4: n_boxes independent Zel'dovich boxes, sides log-uniform in
+    [lo, hi], each on its own mesh; one batch step (graph replay: every box's
+    sort + long-range solve concurrently, one interpolation launch, one
+    persistent PP + kick launch, kick shape autotuned) against the same boxes
+    through the plain single-box path one after another."""
+    import torch
+    from tigerpm_b200 import workloads as W
+    from tigerpm_b200.api import Batch
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    sides, sets = W.ensemble(n_boxes, lo, hi, seed=args.seed + 40 + rank)
+    opts = ensemble_opts(sides)
+    total = int(sum(s.n for s in sets))
+    b = Batch(opts, [s.n for s in sets])
+    for i, ps in enumerate(sets):
+        b.set_input(i, ps)
+    ext = torch.cuda.ExternalStream(b.stream(), device=dev)
+
+    def timed(fn, steps):
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        b.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        for _ in range(steps):
+            fn()
+        e1.record(ext)
+        e1.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), dist, dev)
+
+    b.step(restore=True, graph=False)
+    b.synchronize()
+    shape = b.autotune(repeats=2)
+    for _ in range(args.warmup):
+        b.step(restore=True, graph=True)
+    l0 = b.launch_count()
+    ms = timed(lambda: b.step(restore=True, graph=True), args.steps)
+    launches = (b.launch_count() - l0) // args.steps
+    phases = b.phase_times()
+    for _ in range(max(1, args.warmup // 2)):
+        b.steps_sequential(restore=True)
+    ms_seq = timed(lambda: b.steps_sequential(restore=True), args.steps)
+    b.step(restore=True, graph=True)
+    b.synchronize()
+    acc = None
+    if args.ewald_samples:
+        picks = sorted(set([0, n_boxes // 3, 2 * n_boxes // 3, n_boxes - 1]))
+        acc = ensemble_accuracy([(j, b.box(j)) for j in picks], sets, 256, args.seed + 11)
+    b.close()
+    v = total * world * args.steps / (ms * 1e-3)
+    v_seq = total * world * args.steps / (ms_seq * 1e-3)
+    return {"config": f"{n_boxes} Zel'dovich boxes, sides log-uniform in [{lo}, {hi}] (seeded), "
+                      f"each on its own cloud4 mesh >= 3 points per particle spacing, r_s = 2/3 spacing, "
+                      f"cutoff 6 r_s; {total} particles in all",
+            "sides": [int(s) for s in sides], "meshes": [int(o.four_dim) for o in opts], "particles": total,
+            "value": v, "ms_per_step": ms / args.steps, "gpu_launches_per_step": int(launches),
+            "api": "tpm_batch_step (restore + CUDA graph replay)", "phases_ms": {k: round(x, 4) for k, x in phases.items()},
+            "kick_shape": shape,
+            "sequential": {"value": v_seq, "ms_per_step": ms_seq / args.steps,
+                           "api": "tpm_batch_steps_sequential (plain single-box path, box after box)"},
+            "speedup_vs_sequential": round(ms_seq / ms, 3), "accuracy": acc}
+
+
 def read_traffic(name):
     """DRAM bytes per kick launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", f"kick_pme_{name}.md")
@@ -295,14 +391,13 @@ def read_traffic(name):
 
 
 # ---------------------------------------------------------- CPU (oracle) arm
-def cpu_estimate(cfg, opts, ps, threads, budget_s):
+def cpu_full_kick(cfg, opts, ps, threads):
     """Seconds for one whole kick of the workload on the host cores with the
-    oracle: sort, deposit, FFT + Green + inverse FFT timed in full; the PP +
-    interpolation + kick timed on a random sample of sink cells sized to
-    ~budget_s and extrapolated by candidate-pair counts."""
+    oracle (the CPU restatement of the reference path): chain-mesh sort,
+    deposit + FFT + Green + inverse FFT, and interpolation + PP + rung kick of
+    every particle, each timed as it runs (nothing extrapolated)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    from tigerpm_b200 import workloads as W
     p = O.Particles(*(np.array(a, copy=True) for a in ps.arrays()))
     C_, N = opts.chain_dim, opts.four_dim
     t = time.perf_counter()
@@ -312,38 +407,15 @@ def cpu_estimate(cfg, opts, ps, threads, budget_s):
     phi = O.gravity_long(N, cfg["rs_cells"], {"cloud4": 0, "cic": 1, "tsc": 2}[cfg["assign"]], p.x, p.y, p.z,
                          nthreads=threads)
     t_long = time.perf_counter() - t
-    counts = (pe - pb).astype(np.int64).reshape(C_, C_, C_)
-    nb = np.zeros_like(counts)
-    for dz in (-1, 0, 1):
-        for dy in (-1, 0, 1):
-            for dx in (-1, 0, 1):
-                nb += np.roll(counts, (dz, dy, dx), axis=(0, 1, 2))
-    cand_total = float(np.sum(counts * nb))
     kp = O.KickParams(N=N, C=C_, rs=opts.rs, GM=opts.GM, eta=opts.eta, hsoft=opts.hsoft,
                       rcut=opts.rcut_over_rs * opts.rs, min_rung=0, scale=1.0, t0=1.0, first_call=1, precision=0)
-    g = W.rng(12345)
-    order = g.permutation(C_ ** 3).astype(np.int32)
-    ncell = 8
-    t_pp = 0.0
-    cand_s = 0.0
-    used = 0
     phi32 = phi.astype(np.float32)
-    while used < order.size:
-        cells = order[used:used + ncell]
-        t = time.perf_counter()
-        _, _, _, _, cnt, _ = O.kick_pme(kp, p, pb, pe, phi32, sink_cells=cells, nthreads=threads)
-        t_pp += time.perf_counter() - t
-        cand_s += float(cnt[0])
-        used += cells.size
-        if t_pp > budget_s:
-            break
-        ncell = min(ncell * 2, order.size - used)
-    t_kick = t_pp * cand_total / max(cand_s, 1.0)
+    t = time.perf_counter()
+    _, _, _, _, cnt, _ = O.kick_pme(kp, p, pb, pe, phi32, nthreads=threads)
+    t_kick = time.perf_counter() - t
     total = t_sort + t_long + t_kick
-    sample = (f"sort + deposit + FFT/Green/iFFT timed in full; PP+interp+kick timed on {used} of {C_**3} "
-              f"sink cells ({100.0 * cand_s / cand_total:.2f}% of candidate pairs) and extrapolated by pair count")
-    return total, {"sort_s": round(t_sort, 3), "long_range_s": round(t_long, 3), "kick_s_extrapolated": round(t_kick, 3),
-                   "kick_sample_s": round(t_pp, 3)}, sample
+    return total, {"sort_s": round(t_sort, 3), "long_range_s": round(t_long, 3), "kick_s": round(t_kick, 3),
+                   "pairs_candidate": int(cnt[0]), "pairs_in_cutoff": int(cnt[1])}
 
 
 def cpu_threads():
@@ -365,6 +437,7 @@ def main():
     ap.add_argument("--ewald-samples", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-named", action="store_true", help="skip the literal c2 secondary measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble secondary measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -378,15 +451,25 @@ def main():
         opts = host_opts(cfg)
         ps = make_particles(cfg, args.seed)
         th = cpu_threads()
-        times = []
-        for i in range(args.warmup + args.steps):
-            tt, parts, sample = cpu_estimate(cfg, opts, ps, th, budget_s=2.0)
-            if i >= args.warmup:
-                times.append(tt)
+        # Whole kicks, each timed in full.  A CPU kick of the headline box
+        # takes tens of seconds, so at most one warm-up kick runs and the
+        # timed kicks stop once ~REF_BUDGET_S is spent; `steps` is the number
+        # actually timed (steps_requested keeps what was asked).
+        for _ in range(min(args.warmup, 1)):
+            cpu_full_kick(cfg, opts, ps, th)
+        times, parts = [], None
+        t_all = time.perf_counter()
+        while len(times) < args.steps:
+            tt, parts = cpu_full_kick(cfg, opts, ps, th)
+            times.append(tt)
+            if time.perf_counter() - t_all + tt > REF_BUDGET_S:
+                break
         sec = statistics.mean(times)
         v = ps.n / sec
+        sample = f"{len(times)} whole kicks of all {ps.n} particles, each timed in full"
         line = {"metric": METRIC, "value": v, "unit": "particle-kicks/s", "impl": "reference",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+                "n_gpus": args.gpus, "steps": len(times), "steps_requested": args.steps,
+                "warmup": min(args.warmup, 1), "ms_per_step": sec * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": workload_desc(args.config, cfg, opts),
                 "cpu_baseline": {"value": v, "unit": "particle-kicks/s", "cores": th, "kind": "port",
@@ -402,10 +485,15 @@ def main():
         dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = dist_mod
     res = gpu_arm(args, cfg, args.config, rank, world, dist)
-    named = None
+    batch = None
+    if args.config == "c2-accurate" and not args.no_batch:
+        batch = batch_arm(args, rank, world, dist)
+    named = {}
     if args.config == "c2-accurate" and not args.no_named:
-        ncfg = CONFIGS["c2"]
-        named = gpu_arm(args, ncfg, "c2", rank, world, dist)
+        # the configurations' literal forms, measured in the same run: the
+        # 256^3 Zel'dovich box on its own 256^3 TSC mesh, and the 64^3 box
+        for nm in ("c2", "c1"):
+            named[nm] = gpu_arm(args, CONFIGS[nm], nm, rank, world, dist)
     if rank == 0:
         opts = make_opts(cfg)
         line = {"metric": METRIC, "value": res["value"], "unit": "particle-kicks/s", "n_gpus": world,
@@ -415,17 +503,22 @@ def main():
                 "config": dict(workload_desc(args.config, cfg, opts), parallelism=f"replicas x{world}"),
                 "e2e": res["e2e"], "roofline": res["roofline"], "gpu_launches": res["gpu_launches"],
                 "clocks": res["clocks"], "stages_ms": res["stages_ms"], "accuracy": res.get("accuracy")}
-        if named is not None:
-            line["named_config"] = {"config": workload_desc("c2", CONFIGS["c2"], make_opts(CONFIGS["c2"])),
-                                    "value": named["value"], "ms_per_step": named["ms_per_step"],
-                                    "e2e": named["e2e"]["value"], "accuracy": named.get("accuracy"),
-                                    "stages_ms": named["stages_ms"], "roofline_frac": named["roofline"]["frac"]}
+        if batch is not None:
+            batch["vs_plain_single_box"] = round(batch["value"] / res["value"], 4)
+            line["batch"] = batch
+        for nm, r in named.items():
+            entry = {"config": workload_desc(nm, CONFIGS[nm], make_opts(CONFIGS[nm])),
+                     "value": r["value"], "ms_per_step": r["ms_per_step"], "e2e": r["e2e"]["value"],
+                     "accuracy": r.get("accuracy"), "stages_ms": r["stages_ms"],
+                     "roofline_frac": r["roofline"]["frac"]}
+            line["named_config" if nm == "c2" else f"named_config_{nm}"] = entry
         if world == 1 and not args.no_cpu_baseline:
             ps = make_particles(cfg, args.seed)
             th = cpu_threads()
-            sec, parts, sample = cpu_estimate(cfg, opts, ps, th, budget_s=8.0)
+            sec, parts = cpu_full_kick(cfg, opts, ps, th)
             line["cpu_baseline"] = {"value": ps.n / sec, "unit": "particle-kicks/s", "cores": th, "kind": "port",
-                                    "sample": sample, "stages_s": parts}
+                                    "sample": f"one whole kick of all {ps.n} particles, timed in full",
+                                    "stages_s": parts}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

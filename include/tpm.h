@@ -318,6 +318,137 @@ int tpm_pme_steps_host(tpm_ctx* ctx, int64_t nsteps, int64_t n, const tpm_host_p
  * step beyond 2^31 box lengths. */
 int tpm_check_errors(tpm_ctx* ctx);
 
+/* ------------------------------------------------------------ batches
+ *
+ * An ensemble of independent periodic boxes (each with its own particle
+ * count, PM mesh and chain mesh) kicked together.  The reference kicks one
+ * box per kick_pme call, with a static contiguous split of the box's cells
+ * over the launch (src/kick_pme.cu:139-141) and box splitting when device
+ * memory is short (src/kick_pme.cu:418-430).  A batch step runs every box's
+ * chain-mesh sort and long-range solve concurrently (one stream per box),
+ * then the interpolation of all boxes in one launch and the PP sum + rung
+ * kick of all boxes in ONE persistent launch over a work queue of
+ * (box, chain cell) items ordered heaviest first.  Each box is a tpm_ctx
+ * reachable through tpm_batch_box (results, forces, particles). */
+typedef struct tpm_batch tpm_batch;
+
+/* Launch shape of the kick kernel: warps per block, sources staged in
+ * shared memory per chunk, sinks per pass (a power of two); tuned = 1 when
+ * it came from tpm_batch_autotune; ms = its measured kick time. */
+typedef struct tpm_kick_shape {
+  int warps;
+  int stage;
+  int npass;
+  int tuned;
+  float ms;
+} tpm_kick_shape;
+
+/* Device times of the phases of the last tpm_batch_step, milliseconds. */
+typedef struct tpm_batch_times {
+  float long_range_ms; /* fork: every box's sort + deposit + FFT solve */
+  float queue_ms;      /* work-queue build */
+  float interp_ms;     /* long-range interpolation, all boxes */
+  float kick_ms;       /* persistent PP + rung kick, all boxes */
+} tpm_batch_times;
+
+#define TPM_BATCH_RESTORE 1 /* restore every box's particles from its input first */
+#define TPM_BATCH_GRAPH 2   /* capture the step as a CUDA graph once, replay it */
+
+/* nbox boxes; box i gets options opts[i] and room for capacity[i] particles. */
+int tpm_batch_create(int nbox, const tpm_options* opts, const int64_t* capacity, tpm_batch** out);
+int tpm_batch_destroy(tpm_batch* b);
+int tpm_batch_size(const tpm_batch* b, int* nbox, int64_t* particles);
+/* The context of box i (owned by the batch). */
+int tpm_batch_box(tpm_batch* b, int i, tpm_ctx** ctx);
+/* Host particles of box i: they become its current particles and its
+ * input, which TPM_BATCH_RESTORE copies back before a step. */
+int tpm_batch_set_input(tpm_batch* b, int i, int64_t n, const uint32_t* x, const uint32_t* y, const uint32_t* z,
+                        const float* vx, const float* vy, const float* vz, const int8_t* rung);
+/* One PME kick of every box: chainmesh_create + gravity_long_compute(PME) +
+ * kick_pme over the interior box, per box, with the arguments of
+ * tpm_pme_step.  No host synchronisation. */
+int tpm_batch_step(tpm_batch* b, int flags, int min_rung, double scale, double t0, int first_call);
+/* The same step through the plain single-box path, box after box. */
+int tpm_batch_steps_sequential(tpm_batch* b, int restore_inputs, int min_rung, double scale, double t0,
+                               int first_call);
+int tpm_batch_synchronize(tpm_batch* b);
+/* The batch's main stream (a cudaStream_t): a step ends there. */
+int tpm_batch_stream(tpm_batch* b, void** stream);
+/* This library's kernel launches issued by the batch's steps so far
+ * (a graph replay counts its kernel nodes). */
+int tpm_batch_launch_count(const tpm_batch* b, int64_t* count);
+int tpm_batch_phase_times(tpm_batch* b, tpm_batch_times* out);
+int tpm_batch_get_shape(const tpm_batch* b, tpm_kick_shape* s);
+int tpm_batch_set_shape(tpm_batch* b, const tpm_kick_shape* s);
+/* Times the candidate kick shapes on the batch (after a step) and keeps the
+ * fastest; later batches with the same mean chain-cell occupancy start from
+ * it.  Velocities and rungs are restored; forces are those of a trial. */
+int tpm_batch_autotune(tpm_batch* b, int min_rung, int repeats, tpm_kick_shape* best);
+
+/* ------------------------------------------------------------ serving
+ *
+ * A request loop for kick + drift steps of many resident boxes.  The
+ * reference allocates, stages, kicks and frees per kick_pme call
+ * (src/kick_pme.cu:390-621) and splits a box when free memory is short
+ * (:418-430).  A server keeps each admitted box resident on the device
+ * (particles, chain-mesh tables, FFT twiddles and Green's-function tables,
+ * about 25 bytes per particle) and lends every running step its working set
+ * (forces, packed positions, sort scratch, PM meshes) from a stream-ordered
+ * pool, within one device budget:
+ *     resident bytes of all boxes + working sets of steps in flight <= budget.
+ * Requests queue in FIFO order and start as slots (streams) and memory free
+ * up, so steps of different boxes overlap on the GPU; a dispatcher thread
+ * admits them.  One step = chainmesh_create + gravity_long_compute(PME) +
+ * kick_pme over the whole box + tpm_drift(dt). */
+typedef struct tpm_server tpm_server;
+
+typedef struct tpm_serve_result {
+  int status;        /* TPM_OK or the step's error */
+  int box;
+  double latency_ms; /* submission to completion, host clock */
+  double queue_ms;   /* submission to start (admission wait) */
+  float device_ms;   /* the step's kernels, device clock */
+  int64_t particles; /* particles kicked */
+} tpm_serve_result;
+
+typedef struct tpm_serve_stats_t {
+  int64_t budget_bytes;
+  int64_t resident_bytes;        /* held by admitted boxes */
+  int64_t inflight_peak_bytes;   /* largest sum of working sets in flight */
+  int64_t max_working_set_bytes; /* largest working set of any box */
+  int boxes;
+  int max_concurrent_steps;
+  int64_t steps_done;
+  int64_t particles_done;
+  int64_t launches; /* this library's kernel launches of the served steps */
+} tpm_serve_stats_t;
+
+/* budget_bytes <= 0: 80 % of the device's free memory.  max_slots: steps
+ * in flight at most (1..64). */
+int tpm_serve_create(int64_t budget_bytes, int max_slots, tpm_server** out);
+int tpm_serve_destroy(tpm_server* s);
+/* Admits a box of n particles (host arrays, as tpm_set_particles) with its
+ * options; TPM_ERR_BUDGET when its resident set, with the largest working
+ * set of any box, would not fit the budget. */
+int tpm_serve_add_box(tpm_server* s, const tpm_options* opts, int64_t n, const uint32_t* x, const uint32_t* y,
+                      const uint32_t* z, const float* vx, const float* vy, const float* vz, const int8_t* rung,
+                      int* box_id);
+/* Queues one step of a box (tpm_pme_step arguments + drift dt); returns at once. */
+int tpm_serve_submit(tpm_server* s, int box, double dt, int min_rung, double scale, double t0, int first_call,
+                     int* req_id);
+/* Blocks until the request is done; returns its status. */
+int tpm_serve_wait(tpm_server* s, int req, tpm_serve_result* out);
+/* Blocks until every queued request is done. */
+int tpm_serve_drain(tpm_server* s);
+/* Submits request i for box[i] at arrival_s[i] seconds after the call
+ * starts (host clock), then waits for all; results[i] per request. */
+int tpm_serve_replay(tpm_server* s, int nreq, const int* box, const double* arrival_s, double dt, int min_rung,
+                     double scale, double t0, int first_call, tpm_serve_result* results);
+/* The context of an idle box (its particles, chain mesh offsets); TPM_ERR_STATE
+ * while a step of it is in flight.  Its working set is not kept between steps. */
+int tpm_serve_box(tpm_server* s, int box, tpm_ctx** ctx);
+int tpm_serve_stats(tpm_server* s, tpm_serve_stats_t* out);
+
 /* Candidate sink-source pairs of the 27-cell neighbourhoods (active sinks,
  * rung >= min_rung) and the pairs inside the cutoff, counted on the device. */
 int tpm_count_pairs(tpm_ctx* ctx, int min_rung, int64_t* candidates, int64_t* inside);

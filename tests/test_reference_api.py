@@ -9,6 +9,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INC = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(ROOT, "tigerpm_b200")
 NVCC = "/usr/local/cuda/bin/nvcc"
+REF = os.environ.get("REF", "/root/reference")  # the reference source tree, when mounted
 
 
 def build_driver(tmp_path):
@@ -24,14 +25,14 @@ def test_driver_compiles(tmp_path):
     assert os.path.exists(build_driver(tmp_path))
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="reference tree not mounted")
+@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not mounted")
 def test_shim_matches_reference_headers(tmp_path):
     """reference_api.cpp type-checks against the reference's own headers
     (TPM_REFERENCE_GLOBALS_EXTERNAL), i.e. it defines exactly the functions
     the reference declares."""
     out = str(tmp_path / "ref_api.o")
     subprocess.run([NVCC, "-std=c++17", "-x", "cu", "-c", os.path.join(ROOT, "tigerpm_b200", "csrc", "reference_api.cpp"),
-                    "-DTPM_REFERENCE_GLOBALS_EXTERNAL", "-I/root/reference", "-I" + INC, "-include", "string",
+                    "-DTPM_REFERENCE_GLOBALS_EXTERNAL", "-I" + REF, "-I" + INC, "-include", "string",
                     "-o", out], check=True)
     assert os.path.exists(out)
 

@@ -8,6 +8,10 @@ tpm_gravity_short_ewald (method 1), which uses freshly allocated scratch.
 This file is collected last on purpose: a run that stops at the first failure
 has run every other test before it."""
 import ctypes as C
+import os
+import subprocess
+import sys
+import textwrap
 
 import numpy as np
 import pytest
@@ -58,6 +62,76 @@ def test_noalloc_ewald_matches_allocating_path_twice():
         assert np.all(np.isfinite(phi)) and np.all(np.isfinite(g))
         assert rel_rms(phi, rphi) < 1e-9
         assert rel_rms(g, rg) < 1e-9
+
+
+def _call(lib, torch, src, n, snk, out, stream, hsoft):
+    rc = lib.tpm_ewald_fp64_noalloc(*[C.c_void_p(a.data_ptr()) for a in src], n,
+                                    *[C.c_void_p(a.data_ptr()) for a in snk], int(snk[0].numel()), hsoft,
+                                    *[C.c_void_p(o.data_ptr()) for o in out], stream)
+    _lib.check(rc, "tpm_ewald_fp64_noalloc")
+
+
+def test_noalloc_ewald_allocates_nothing():
+    """After a first call (which only looks up the library's buffer), further
+    calls on other sinks leave the device's free memory and torch's allocator
+    untouched."""
+    import torch
+    lib = _lib.load()
+    ps = particle_set("uniform", 16, 43)
+    src = [_dev(torch, a) for a in (ps.x, ps.y, ps.z)]
+    snk = [_dev(torch, a[:64]) for a in (ps.x, ps.y, ps.z)]
+    snk2 = [_dev(torch, a[100:131]) for a in (ps.x, ps.y, ps.z)]
+    out = [torch.empty(64, dtype=torch.float64, device="cuda") for _ in range(4)]
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _call(lib, torch, src, ps.n, snk, out, stream, 0.01)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    stats0 = torch.cuda.memory_stats()
+    for _ in range(3):
+        _call(lib, torch, src, ps.n, snk2, [o[:31] for o in out], stream, 0.01)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    stats1 = torch.cuda.memory_stats()
+    assert free1 == free0
+    for k in ("allocation.all.allocated", "segment.all.allocated", "reserved_bytes.all.allocated"):
+        assert stats1.get(k, 0) == stats0.get(k, 0), k
+
+
+def test_noalloc_ewald_first_call_on_nonblocking_stream():
+    """The very first call in a process, queued on a non-blocking stream,
+    already sees the reciprocal-vector table its set-up copies."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = textwrap.dedent("""
+        import ctypes as C, sys
+        import numpy as np, torch
+        sys.path.insert(0, %r); sys.path.insert(0, %r)
+        from tigerpm_b200 import _lib
+        from helpers import particle_set, rel_rms
+        from tigerpm_b200.api import TigerPM, make_options
+        lib = _lib.load()
+        ps = particle_set("halos", 16, 47)
+        sx, sy, sz = ps.x[:50].copy(), ps.y[:50].copy(), ps.z[:50].copy()
+        s = torch.cuda.Stream()  # created with cudaStreamNonBlocking
+        src = [torch.from_numpy(a).cuda() for a in (ps.x, ps.y, ps.z)]
+        snk = [torch.from_numpy(a).cuda() for a in (sx, sy, sz)]
+        out = [torch.empty(50, dtype=torch.float64, device="cuda") for _ in range(4)]
+        torch.cuda.synchronize()
+        rc = lib.tpm_ewald_fp64_noalloc(*[C.c_void_p(a.data_ptr()) for a in src], ps.n,
+                                        *[C.c_void_p(a.data_ptr()) for a in snk], 50, 0.005,
+                                        *[C.c_void_p(o.data_ptr()) for o in out], C.c_void_p(s.cuda_stream))
+        _lib.check(rc, "noalloc")
+        s.synchronize()
+        opts = make_options(16, 16, rs_cells=1.0)
+        opts.hsoft = 0.005
+        with TigerPM(opts, ps.n) as t:
+            t.set_particles(ps)
+            phi, g = t.gravity_short_ewald_call_kernel(sx, sy, sz, method=1)
+        assert rel_rms(out[0].cpu().numpy(), phi) < 1e-9
+        assert rel_rms(torch.stack(out[1:], 1).cpu().numpy(), np.stack(g, 1)) < 1e-9
+        print("ok")
+    """) % (root, os.path.join(root, "tests"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
 
 
 def test_noalloc_ewald_rejects_too_many_sinks():

@@ -59,6 +59,33 @@ class HostParticles(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("x", "y", "z", "vx", "vy", "vz", "rung")]
 
 
+class KickShape(C.Structure):
+    """struct tpm_kick_shape."""
+    _fields_ = [("warps", C.c_int), ("stage", C.c_int), ("npass", C.c_int), ("tuned", C.c_int), ("ms", C.c_float)]
+
+
+class BatchTimes(C.Structure):
+    """struct tpm_batch_times."""
+    _fields_ = [(n, C.c_float) for n in ("long_range_ms", "queue_ms", "interp_ms", "kick_ms")]
+
+
+class ServeResult(C.Structure):
+    """struct tpm_serve_result."""
+    _fields_ = [("status", C.c_int), ("box", C.c_int), ("latency_ms", C.c_double), ("queue_ms", C.c_double),
+                ("device_ms", C.c_float), ("particles", C.c_int64)]
+
+
+class ServeStats(C.Structure):
+    """struct tpm_serve_stats_t."""
+    _fields_ = [("budget_bytes", C.c_int64), ("resident_bytes", C.c_int64), ("inflight_peak_bytes", C.c_int64),
+                ("max_working_set_bytes", C.c_int64), ("boxes", C.c_int), ("max_concurrent_steps", C.c_int),
+                ("steps_done", C.c_int64), ("particles_done", C.c_int64), ("launches", C.c_int64)]
+
+
+BATCH_RESTORE = 1
+BATCH_GRAPH = 2
+
+
 class DeviceArrays(C.Structure):
     _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p), ("vx", C.c_void_p),
                 ("vy", C.c_void_p), ("vz", C.c_void_p), ("rung", C.c_void_p), ("gx", C.c_void_p),
@@ -109,6 +136,29 @@ SIGNATURES = [
     ("tpm_pme_step", _I, [_P, _I, _D, _D, _I]),
     ("tpm_pme_steps_host", _I, [_P, _I64, _I64, _P, _P, _I, _D, _D, _I]),
     ("tpm_check_errors", _I, [_P]),
+    ("tpm_batch_create", _I, [_I, C.POINTER(Options), C.POINTER(_I64), C.POINTER(_P)]),
+    ("tpm_batch_destroy", _I, [_P]),
+    ("tpm_batch_size", _I, [_P, C.POINTER(_I), C.POINTER(_I64)]),
+    ("tpm_batch_box", _I, [_P, _I, C.POINTER(_P)]),
+    ("tpm_batch_set_input", _I, [_P, _I, _I64, _P, _P, _P, _P, _P, _P, _P]),
+    ("tpm_batch_step", _I, [_P, _I, _I, _D, _D, _I]),
+    ("tpm_batch_steps_sequential", _I, [_P, _I, _I, _D, _D, _I]),
+    ("tpm_batch_synchronize", _I, [_P]),
+    ("tpm_batch_stream", _I, [_P, C.POINTER(_P)]),
+    ("tpm_batch_launch_count", _I, [_P, C.POINTER(_I64)]),
+    ("tpm_batch_phase_times", _I, [_P, C.POINTER(BatchTimes)]),
+    ("tpm_batch_get_shape", _I, [_P, C.POINTER(KickShape)]),
+    ("tpm_batch_set_shape", _I, [_P, C.POINTER(KickShape)]),
+    ("tpm_batch_autotune", _I, [_P, _I, _I, C.POINTER(KickShape)]),
+    ("tpm_serve_create", _I, [_I64, _I, C.POINTER(_P)]),
+    ("tpm_serve_destroy", _I, [_P]),
+    ("tpm_serve_add_box", _I, [_P, C.POINTER(Options), _I64, _P, _P, _P, _P, _P, _P, _P, C.POINTER(_I)]),
+    ("tpm_serve_submit", _I, [_P, _I, _D, _I, _D, _D, _I, C.POINTER(_I)]),
+    ("tpm_serve_wait", _I, [_P, _I, C.POINTER(ServeResult)]),
+    ("tpm_serve_drain", _I, [_P]),
+    ("tpm_serve_replay", _I, [_P, _I, _P, _P, _D, _I, _D, _D, _I, _P]),
+    ("tpm_serve_box", _I, [_P, _I, C.POINTER(_P)]),
+    ("tpm_serve_stats", _I, [_P, C.POINTER(ServeStats)]),
     ("tpm_count_pairs", _I, [_P, _I, C.POINTER(_I64), C.POINTER(_I64)]),
     ("tpm_fp32_peak_probe", _I, [C.POINTER(_D)]),
 ]

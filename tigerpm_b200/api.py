@@ -133,11 +133,25 @@ class TigerPM:
         self.h = h
         self.capacity = int(capacity)
         self.n = 0
+        self.owned = True
+
+    @classmethod
+    def borrow(cls, handle, opts: Options, n: int) -> "TigerPM":
+        """A view of a context owned elsewhere (a batch's box); close() does
+        not destroy it."""
+        t = cls.__new__(cls)
+        t.lib = _lib.load()
+        t.opts = opts
+        t.h = handle
+        t.capacity = int(n)
+        t.n = int(n)
+        t.owned = False
+        return t
 
     def close(self):
-        if self.h:
+        if self.h and self.owned:
             self.lib.tpm_ctx_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -359,6 +373,183 @@ class TigerPM:
         b = C.c_int64()
         check(self.lib.tpm_count_pairs(self.h, int(min_rung), C.byref(a), C.byref(b)), "count_pairs")
         return int(a.value), int(b.value)
+
+
+class Batch:
+    """An ensemble of independent periodic boxes kicked together
+    (tpm_batch_*): every box's sort and long-range solve run concurrently,
+    then one interpolation launch and ONE persistent PP + kick launch over a
+    (box, chain cell) work queue, optionally captured as a CUDA graph."""
+
+    def __init__(self, opts_list, capacities):
+        self.lib = _lib.load()
+        nb = len(opts_list)
+        if nb == 0 or len(capacities) != nb:
+            raise ValueError("one capacity per box")
+        self.opts = list(opts_list)
+        arr = (Options * nb)(*opts_list)
+        caps = (C.c_int64 * nb)(*[int(c) for c in capacities])
+        h = C.c_void_p()
+        check(self.lib.tpm_batch_create(nb, arr, caps, C.byref(h)), "batch_create")
+        self.h = h
+        self.nbox = nb
+        self.counts = [0] * nb
+
+    def close(self):
+        if self.h:
+            self.lib.tpm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_input(self, i: int, ps) -> None:
+        x, y, z, vx, vy, vz, r = (np.ascontiguousarray(a) for a in
+                                  (ps.x, ps.y, ps.z, ps.vx, ps.vy, ps.vz, ps.rung))
+        check(self.lib.tpm_batch_set_input(self.h, int(i), x.size, _ptr(x), _ptr(y), _ptr(z), _ptr(vx), _ptr(vy),
+                                           _ptr(vz), _ptr(r)), "batch_set_input")
+        self.counts[i] = int(x.size)
+
+    def box(self, i: int) -> TigerPM:
+        """The context of box i (owned by the batch)."""
+        h = C.c_void_p()
+        check(self.lib.tpm_batch_box(self.h, int(i), C.byref(h)), "batch_box")
+        return TigerPM.borrow(h, self.opts[i], self.counts[i])
+
+    def step(self, restore: bool = True, graph: bool = True, min_rung: int = 0, scale: float = 1.0,
+             t0: float = 1.0, first_call: bool = True) -> None:
+        flags = (_lib.BATCH_RESTORE if restore else 0) | (_lib.BATCH_GRAPH if graph else 0)
+        check(self.lib.tpm_batch_step(self.h, flags, int(min_rung), float(scale), float(t0),
+                                      1 if first_call else 0), "batch_step")
+
+    def steps_sequential(self, restore: bool = True, min_rung: int = 0, scale: float = 1.0, t0: float = 1.0,
+                         first_call: bool = True) -> None:
+        check(self.lib.tpm_batch_steps_sequential(self.h, 1 if restore else 0, int(min_rung), float(scale),
+                                                  float(t0), 1 if first_call else 0), "batch_steps_sequential")
+
+    def synchronize(self) -> None:
+        check(self.lib.tpm_batch_synchronize(self.h), "batch_synchronize")
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        check(self.lib.tpm_batch_stream(self.h, C.byref(p)), "batch_stream")
+        return int(p.value or 0)
+
+    def launch_count(self) -> int:
+        v = C.c_int64()
+        check(self.lib.tpm_batch_launch_count(self.h, C.byref(v)), "batch_launch_count")
+        return int(v.value)
+
+    def phase_times(self) -> dict:
+        t = _lib.BatchTimes()
+        check(self.lib.tpm_batch_phase_times(self.h, C.byref(t)), "batch_phase_times")
+        return {n: float(getattr(t, n)) for n, _ in _lib.BatchTimes._fields_}
+
+    def shape(self) -> dict:
+        k = _lib.KickShape()
+        check(self.lib.tpm_batch_get_shape(self.h, C.byref(k)), "batch_get_shape")
+        return {n: getattr(k, n) for n, _ in _lib.KickShape._fields_}
+
+    def set_shape(self, warps: int, stage: int, npass: int) -> None:
+        k = _lib.KickShape(warps, stage, npass, 0, 0.0)
+        check(self.lib.tpm_batch_set_shape(self.h, C.byref(k)), "batch_set_shape")
+
+    def autotune(self, min_rung: int = 0, repeats: int = 2) -> dict:
+        k = _lib.KickShape()
+        check(self.lib.tpm_batch_autotune(self.h, int(min_rung), int(repeats), C.byref(k)), "batch_autotune")
+        return {n: getattr(k, n) for n, _ in _lib.KickShape._fields_}
+
+
+class Server:
+    """A request loop serving kick + drift steps of resident boxes
+    (tpm_serve_*): boxes are admitted against an HBM budget, requests start
+    as slots and memory free up, and steps of different boxes overlap on the
+    device."""
+
+    def __init__(self, budget_bytes: int = 0, max_slots: int = 4):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.tpm_serve_create(int(budget_bytes), int(max_slots), C.byref(h)), "serve_create")
+        self.h = h
+        self.opts = []
+        self.counts = []
+
+    def close(self):
+        if self.h:
+            self.lib.tpm_serve_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add_box(self, opts: Options, ps) -> int:
+        x, y, z, vx, vy, vz, r = (np.ascontiguousarray(a) for a in
+                                  (ps.x, ps.y, ps.z, ps.vx, ps.vy, ps.vz, ps.rung))
+        bid = C.c_int()
+        check(self.lib.tpm_serve_add_box(self.h, C.byref(opts), x.size, _ptr(x), _ptr(y), _ptr(z), _ptr(vx),
+                                         _ptr(vy), _ptr(vz), _ptr(r), C.byref(bid)), "serve_add_box")
+        self.opts.append(opts)
+        self.counts.append(int(x.size))
+        return int(bid.value)
+
+    def submit(self, box: int, dt: float, min_rung: int = 0, scale: float = 1.0, t0: float = 1.0,
+               first_call: bool = True) -> int:
+        rid = C.c_int()
+        check(self.lib.tpm_serve_submit(self.h, int(box), float(dt), int(min_rung), float(scale), float(t0),
+                                        1 if first_call else 0, C.byref(rid)), "serve_submit")
+        return int(rid.value)
+
+    @staticmethod
+    def _result(r) -> dict:
+        return {n: getattr(r, n) for n, _ in _lib.ServeResult._fields_}
+
+    def wait(self, req: int) -> dict:
+        r = _lib.ServeResult()
+        check(self.lib.tpm_serve_wait(self.h, int(req), C.byref(r)), "serve_wait")
+        return self._result(r)
+
+    def drain(self) -> None:
+        check(self.lib.tpm_serve_drain(self.h), "serve_drain")
+
+    def replay(self, boxes, arrivals_s, dt: float, min_rung: int = 0, scale: float = 1.0, t0: float = 1.0,
+               first_call: bool = True):
+        """Request i for boxes[i] submitted arrivals_s[i] seconds after the
+        call starts; returns one result dict per request."""
+        b = np.ascontiguousarray(boxes, np.int32)
+        a = np.ascontiguousarray(arrivals_s, np.float64)
+        res = (_lib.ServeResult * max(b.size, 1))()
+        check(self.lib.tpm_serve_replay(self.h, int(b.size), _ptr(b), _ptr(a), float(dt), int(min_rung),
+                                        float(scale), float(t0), 1 if first_call else 0, res), "serve_replay")
+        return [self._result(res[i]) for i in range(b.size)]
+
+    def box(self, i: int) -> TigerPM:
+        """The context of an idle box (particles, chain-mesh offsets)."""
+        h = C.c_void_p()
+        check(self.lib.tpm_serve_box(self.h, int(i), C.byref(h)), "serve_box")
+        return TigerPM.borrow(h, self.opts[i], self.counts[i])
+
+    def stats(self) -> dict:
+        s = _lib.ServeStats()
+        check(self.lib.tpm_serve_stats(self.h, C.byref(s)), "serve_stats")
+        return {n: getattr(s, n) for n, _ in _lib.ServeStats._fields_}
 
 
 def fp32_peak_probe() -> float:

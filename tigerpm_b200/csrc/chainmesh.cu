@@ -454,6 +454,25 @@ __global__ void k_gather(int64_t n, const int32_t* __restrict__ idx, const uint3
   pos4[p] = make_int4((int)a, (int)b, (int)c, 0);
 }
 
+// The sorted set back into the current arrays (batch members keep fixed
+// device addresses across steps).
+__global__ void k_copy_back(int64_t n, const uint32_t* __restrict__ x2, const uint32_t* __restrict__ y2,
+                            const uint32_t* __restrict__ z2, const float* __restrict__ vx2,
+                            const float* __restrict__ vy2, const float* __restrict__ vz2,
+                            const int8_t* __restrict__ rung2, uint32_t* __restrict__ x, uint32_t* __restrict__ y,
+                            uint32_t* __restrict__ z, float* __restrict__ vx, float* __restrict__ vy,
+                            float* __restrict__ vz, int8_t* __restrict__ rung) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  x[p] = x2[p];
+  y[p] = y2[p];
+  z[p] = z2[p];
+  vx[p] = vx2[p];
+  vy[p] = vy2[p];
+  vz[p] = vz2[p];
+  rung[p] = rung2[p];
+}
+
 int scan_exclusive(tpm_ctx* c, const int32_t* in, int64_t n, int32_t* out) {
   if (n <= (int64_t)kScanTile * 64) {
     k_scan_single<<<1, kScanThreads, 0, c->stream>>>(in, n, out);
@@ -548,13 +567,20 @@ int chainmesh_sort(tpm_ctx* c) {
                                                c->pos4);
     c->launches++;
     TPM_CUDA_TRY(cudaGetLastError());
-    std::swap(c->x, c->x2);
-    std::swap(c->y, c->y2);
-    std::swap(c->z, c->z2);
-    std::swap(c->vx, c->vx2);
-    std::swap(c->vy, c->vy2);
-    std::swap(c->vz, c->vz2);
-    std::swap(c->rung, c->rung2);
+    if (c->stable_buffers) {
+      k_copy_back<<<ceil_div(n, 256), 256, 0, s>>>(n, c->x2, c->y2, c->z2, c->vx2, c->vy2, c->vz2, c->rung2, c->x,
+                                                   c->y, c->z, c->vx, c->vy, c->vz, c->rung);
+      c->launches++;
+      TPM_CUDA_TRY(cudaGetLastError());
+    } else {
+      std::swap(c->x, c->x2);
+      std::swap(c->y, c->y2);
+      std::swap(c->z, c->z2);
+      std::swap(c->vx, c->vx2);
+      std::swap(c->vy, c->vy2);
+      std::swap(c->vz, c->vz2);
+      std::swap(c->rung, c->rung2);
+    }
   }
   stage_end(c, kStSort);
   c->sorted = true;

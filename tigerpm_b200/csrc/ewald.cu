@@ -339,9 +339,9 @@ int ewald(tpm_ctx* c, int64_t ns, const uint32_t* dsx, const uint32_t* dsy, cons
   stage_begin(c, kStEwald);
   double* buf = nullptr;
   HVec* dhv = nullptr;
-  TPM_CUDA_TRY(cudaMallocAsync((void**)&buf, sizeof(double) * need, c->stream));
-  TPM_CUDA_TRY(cudaMallocAsync((void**)&dhv, sizeof(HVec) * nh, c->stream));
-  cudaError_t e = cudaMemcpyAsync(dhv, hv.data(), sizeof(HVec) * nh, cudaMemcpyHostToDevice, c->stream);
+  cudaError_t e = cudaMallocAsync((void**)&buf, sizeof(double) * need, c->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&dhv, sizeof(HVec) * nh, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dhv, hv.data(), sizeof(HVec) * nh, cudaMemcpyHostToDevice, c->stream);
   EwArgs a;
   a.x = c->x;
   a.y = c->y;
@@ -377,8 +377,8 @@ int ewald(tpm_ctx* c, int64_t ns, const uint32_t* dsx, const uint32_t* dsy, cons
   }
   std::vector<double> host((size_t)4 * ns);
   if (e == cudaSuccess) e = cudaMemcpyAsync(host.data(), out, sizeof(double) * 4 * ns, cudaMemcpyDeviceToHost, c->stream);
-  cudaFreeAsync(buf, c->stream);
-  cudaFreeAsync(dhv, c->stream);
+  if (buf) cudaFreeAsync(buf, c->stream);
+  if (dhv) cudaFreeAsync(dhv, c->stream);
   stage_end(c, kStEwald);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return fail(TPM_ERR_CUDA, std::string("ewald: ") + cudaGetErrorString(e));

@@ -301,6 +301,11 @@ int setup(int dev, DeviceState** out) {
     const cudaError_t e2 =
         cudaMemcpy((unsigned char*)ptr + kOffH, hv.data(), sizeof(HVec) * hv.size(), cudaMemcpyHostToDevice);
     if (e2 != cudaSuccess) return fail(TPM_ERR_CUDA, std::string("reciprocal table: ") + cudaGetErrorString(e2));
+    // A pageable cudaMemcpy may return once the data is staged, before it
+    // lands; kernels on a non-blocking caller stream (or another thread that
+    // sees `ready`) must not read the table early, so wait for the device.
+    const cudaError_t e3 = cudaDeviceSynchronize();
+    if (e3 != cudaSuccess) return fail(TPM_ERR_CUDA, std::string("reciprocal table sync: ") + cudaGetErrorString(e3));
     st.scratch = (unsigned char*)ptr;
     st.nh = (int)hv.size();
     st.ready = true;

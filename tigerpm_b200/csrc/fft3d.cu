@@ -255,6 +255,12 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_z_r2c(const float* __restri
       Y[row * p.Sz + kz] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
       Y[(row + 1) * p.Sz + kz] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
     }
+    // padding columns: zero, so a borrowed (uninitialised) spectrum buffer
+    // carries no stale values through the column passes
+    for (int kz = Nh + threadIdx.x; kz < p.Sz; kz += kFftThreads) {
+      Y[row * p.Sz + kz] = make_float2(0.f, 0.f);
+      Y[(row + 1) * p.Sz + kz] = make_float2(0.f, 0.f);
+    }
   }
 }
 
@@ -419,7 +425,7 @@ int fft3d_init(tpm_ctx* c) {
   }
   TPM_CUDA_TRY(cudaMemcpy(c->fft_tw, tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
   // padding columns stay zero: the transforms keep them zero and never store them into phi
-  TPM_CUDA_TRY(cudaMemset(c->rhok, 0, sizeof(float2) * (size_t)N * N * fft3d_padded_columns(N)));
+  if (c->rhok) TPM_CUDA_TRY(cudaMemset(c->rhok, 0, sizeof(float2) * (size_t)N * N * fft3d_padded_columns(N)));
   const int smem = (int)fft_smem(N);
   TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));

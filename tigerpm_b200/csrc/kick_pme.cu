@@ -72,8 +72,11 @@ struct KickArgs {
   int first_call;
   int kahan;
   float GM, eta, t0, scale, hsoft;
-  float inv2rs, twooversqrtpi, h2, hinv, h3inv, rcut2;
-  float p_r, e_r, c_r;  // A&S p, -log2(e), 2/sqrt(pi), each times powers of 1/(2 r_s)
+  // pair-loop lengths are in units of 2 r_s (see PairK)
+  float inv2rs;  // 1 / (2 r_s), box units
+  float lscale;  // 2^-32 / (2 r_s): fixed32 offset -> scaled length
+  float h2;      // (hsoft / 2 r_s)^2
+  float rcut2;   // (r_cut / 2 r_s)^2, or infinity without a cutoff
 };
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
@@ -155,17 +158,10 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
 // compute it, one block per sink cell, chosen by the mesh points per sink.
 //
 // Direct form: one thread per sink, the 216 points read through L1.
-__global__ void __launch_bounds__(64) k_interp_direct(KickArgs a) {
-  int bid = blockIdx.x;
-  const int i2 = bid % a.s2;
-  bid /= a.s2;
-  const int i1 = bid % a.s1;
-  const int i0 = bid / a.s1;
-  const int C = a.C;
-  const int64_t key = ((int64_t)(a.b2 + i2) * C + (a.b1 + i1)) * C + (a.b0 + i0);
+__device__ __forceinline__ void interp_cell_direct(const KickArgs& a, int64_t key, int min_rung) {
   const int32_t pb = __ldg(a.begin + key), pe = __ldg(a.begin + key + 1);
   for (int32_t i = pb + (int32_t)threadIdx.x; i < pe; i += blockDim.x) {
-    if (a.rung[i] < a.min_rung) continue;
+    if (a.rung[i] < min_rung) continue;
     float lx, ly, lz, lp;
     interp_long(a, __ldg(a.pos4 + i), lx, ly, lz, lp);
     a.gx[i] = lx;
@@ -173,6 +169,16 @@ __global__ void __launch_bounds__(64) k_interp_direct(KickArgs a) {
     a.gz[i] = lz;
     a.pot[i] = lp;
   }
+}
+
+__global__ void __launch_bounds__(64) k_interp_direct(KickArgs a) {
+  int bid = blockIdx.x;
+  const int i2 = bid % a.s2;
+  bid /= a.s2;
+  const int i1 = bid % a.s1;
+  const int i0 = bid / a.s1;
+  const int C = a.C;
+  interp_cell_direct(a, ((int64_t)(a.b2 + i2) * C + (a.b1 + i1)) * C + (a.b0 + i0), a.min_rung);
 }
 
 // The same interpolation from a shared-memory copy of the potential: one
@@ -284,36 +290,51 @@ __global__ void __launch_bounds__(128) k_interp_tile(KickArgs a, int maxw) {
 // offset to the minimum image, as the reference's int32 difference does; it
 // is needed only when chain_dim = 3, where the 27 cells span the whole box
 // and an offset from the cell centre can exceed half the box.
+// Pair constants that stay in registers through the pair loop.  Lengths in
+// the pair loop are in units of 2 r_s, so that the erfc argument
+// x0 = r / (2 r_s) is r itself and the A&S and exp constants are literals:
+// rcut2 and h2 are (r_cut / 2 r_s)^2 and (h / 2 r_s)^2; wrap_len is the box
+// length in those units (minimum-image fold, chain_dim = 3 only).
+struct PairK {
+  float rcut2, h2, wrap_len;
+};
+
+// One source against one sink (src/kick_pme.cu:285-314).  WRAP folds the
+// offset to the minimum image, as the reference's int32 difference does; it
+// is needed only when chain_dim = 3, where the 27 cells span the whole box
+// and an offset from the cell centre can exceed half the box.  Sums are in
+// the scaled units: force x 1/(2 r_s)^2, potential x 1/(2 r_s).
 template <bool WRAP>
-__device__ __forceinline__ void pair(const KickArgs& a, float dx, float dy, float dz, float& gx, float& gy,
-                                     float& gz, float& ph) {
+__device__ __forceinline__ void pair(const PairK& k, float dx, float dy, float dz, float& gx, float& gy, float& gz,
+                                     float& ph) {
   if (WRAP) {
-    dx -= rintf(dx);
-    dy -= rintf(dy);
-    dz -= rintf(dz);
+    const float inv = 1.0f / k.wrap_len;
+    dx -= rintf(dx * inv) * k.wrap_len;
+    dy -= rintf(dy * inv) * k.wrap_len;
+    dz -= rintf(dz * inv) * k.wrap_len;
   }
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   // Pairs beyond the cutoff take r^2 = 1e30: 1/r, erfc and exp(-x^2) then
   // vanish and the pair adds exactly 0, without a mask on the results.
-  const float r2c = r2 < a.rcut2 ? fmaxf(r2, a.h2) : 1e30f;
+  const float r2c = r2 < k.rcut2 ? fmaxf(r2, k.h2) : 1e30f;
   const float rinv = rsqrt_approx(r2c);
   const float r = r2c * rinv;
-  // x0 = r / (2 r_s); the constants carry 1/(2 r_s): p x0 = p_r r,
-  // -log2(e) x0^2 = e_r r^2, (2/sqrt(pi)) x0 = c_r r
-  const float t = rcp_approx(fmaf(a.p_r, r, 1.0f));
-  const float e = ex2_approx(a.e_r * r2c);
+  // A&S 7.1.26 erfc(x0) with x0 = r; exp(-x0^2) = 2^(-log2(e) r^2)
+  const float t = rcp_approx(fmaf(0.3275911f, r, 1.0f));
+  const float e = ex2_approx(-1.4426950408889634f * r2c);
   const float poly =
       t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f), 0.254829592f);
   const float erfc0 = poly * e;
   const float rinv2 = rinv * rinv;
-  float rinv3 = fmaf(a.c_r * r, e, erfc0) * rinv2 * rinv;
+  float rinv3 = fmaf(1.1283791670955126f * r, e, erfc0) * rinv2 * rinv;  // 2/sqrt(pi)
   float rinv1 = erfc0;  // times 1/r below
   float rscale = rinv;
-  if (r2 <= a.h2) {  // softened Newtonian kernel inside hsoft (rare)
-    const float q2 = r2 * a.hinv * a.hinv;
-    rinv3 = fmaf(fmaf(15.0f / 8.0f, q2, -21.0f / 4.0f), q2, 35.0f / 8.0f) * a.h3inv;
+  if (r2 <= k.h2) {  // softened Newtonian kernel inside hsoft (rare)
+    const float hinv = rsqrtf(k.h2);
+    const float q2 = r2 * hinv * hinv;
+    rinv3 = fmaf(fmaf(15.0f / 8.0f, q2, -21.0f / 4.0f), q2, 35.0f / 8.0f) * (hinv * hinv * hinv);
     rinv1 = fmaf(fmaf(fmaf(-5.0f / 16.0f, q2, 21.0f / 16.0f), q2, -35.0f / 16.0f), q2, 35.0f / 16.0f);
-    rscale = a.hinv;
+    rscale = hinv;
   }
   gx = fmaf(-dx, rinv3, gx);
   gy = fmaf(-dy, rinv3, gy);
@@ -321,6 +342,11 @@ __device__ __forceinline__ void pair(const KickArgs& a, float dx, float dy, floa
   ph = fmaf(-rinv1, rscale, ph);
 }
 
+// Offset a - b of two fixed32 coordinates (the reference's int32 wrap-around
+// difference) times a length scale.
+__device__ __forceinline__ float offset_scaled(uint32_t a, uint32_t b, float sc) {
+  return (float)(int32_t)(a - b) * sc;
+}
 
 // 3-bit-per-axis sub-cell index of an offset (in box units) from the cell
 // centre, interleaved into a 9-bit Morton key.
@@ -356,9 +382,11 @@ constexpr int kGroup = 8;
 constexpr int kBuf = 64;
 constexpr int kMaxRuns = 18;
 
+// The whole kick of one sink cell (cx, cy, cz) by the calling block; every
+// thread of the block calls it with the same arguments.
 template <bool WRAP>
-__global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickArgs a, int stage, int npass) {
-  extern __shared__ float4 smem4[];
+__device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int cz, float4* smem4, int stage,
+                                          int npass) {
   const int T = blockDim.x, W = T >> 5;
   float4* src = smem4;
   float4* bufs = src + stage;
@@ -368,12 +396,6 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
   int* runb = reinterpret_cast<int*>(skey + npass);
   int* runp = runb + kMaxRuns;
   const int C = a.C;
-  int bid = blockIdx.x;
-  const int i2 = bid % a.s2;
-  bid /= a.s2;
-  const int i1 = bid % a.s1;
-  const int i0 = bid / a.s1;
-  const int cx = a.b0 + i0, cy = a.b1 + i1, cz = a.b2 + i2;
   const int64_t key = ((int64_t)cz * C + cy) * C + cx;
   const int32_t pb = __ldg(a.begin + key), pe = __ldg(a.begin + key + 1);
   if (pb == pe) return;
@@ -384,6 +406,8 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
   const int t8 = lane & 7, ph = lane >> 3;
   const float Cf = (float)C;
   const bool cull = !WRAP && a.rcut2 < INFINITY;  // culling works on unwrapped offsets
+  const float sc = a.lscale;
+  const PairK pk{a.rcut2, a.h2, a.inv2rs};
   if (tid == 0) {
     int nr = 0, tot = 0;
     for (int dz = -1; dz <= 1; dz++) {
@@ -450,7 +474,8 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
       float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
       if (act) {
         const int4 q = __ldg(a.pos4 + sbase + (int32_t)(m & 0xffu));
-        p = make_float4(distance32((uint32_t)q.x, ox), distance32((uint32_t)q.y, oy), distance32((uint32_t)q.z, oz), 0.f);
+        p = make_float4(offset_scaled((uint32_t)q.x, ox, sc), offset_scaled((uint32_t)q.y, oy, sc),
+                        offset_scaled((uint32_t)q.z, oz, sc), 0.f);
       }
       spos[e] = p;
 #pragma unroll
@@ -469,8 +494,8 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
         int r = 0;
         while (runp[r + 1] <= e) r++;
         const int4 u = __ldg(a.pos4 + runb[r] + (e - runp[r]));
-        src[j] = make_float4(distance32((uint32_t)u.x, ox), distance32((uint32_t)u.y, oy),
-                             distance32((uint32_t)u.z, oz), 0.f);
+        src[j] = make_float4(offset_scaled((uint32_t)u.x, ox, sc), offset_scaled((uint32_t)u.y, oy, sc),
+                             offset_scaled((uint32_t)u.z, oz, sc), 0.f);
       }
       __syncthreads();
       for (int g = warp; g < ngroups; g += W) {
@@ -514,7 +539,7 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
 #pragma unroll
             for (int k = 0; k < 32; k += 4) {
               const float4 u = buf[k + ph];
-              if (mysink) pair<WRAP>(a, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
+              if (mysink) pair<WRAP>(pk, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
             }
             __syncwarp();
             if (lane < cnt - 32) buf[lane] = buf[32 + lane];
@@ -525,7 +550,7 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
         for (int k = 0; k < cnt; k += 4) {
           if (k + ph < cnt && mysink) {
             const float4 u = buf[k + ph];
-            pair<WRAP>(a, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
+            pair<WRAP>(pk, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
           }
         }
         __syncwarp();
@@ -559,10 +584,12 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
       const int32_t i = sbase + (int32_t)(skey[e] & 0xffu);
       const float lx = a.gx[i], ly = a.gy[i], lz = a.gz[i], lp = a.pot[i];  // from k_interp_long
       const float* A = acc + e * 8;
-      const float g0 = ((A[0] - A[4]) + lx) * a.GM;
-      const float g1 = ((A[1] - A[5]) + ly) * a.GM;
-      const float g2 = ((A[2] - A[6]) + lz) * a.GM;
-      const float phi = ((A[3] - A[7]) + lp) * a.GM;
+      // pair sums back from units of 2 r_s: force x (1/2r_s)^2, potential x 1/2r_s
+      const float fs = a.inv2rs * a.inv2rs;
+      const float g0 = fmaf(A[0] - A[4], fs, lx) * a.GM;
+      const float g1 = fmaf(A[1] - A[5], fs, ly) * a.GM;
+      const float g2 = fmaf(A[2] - A[6], fs, lz) * a.GM;
+      const float phi = fmaf(A[3] - A[7], a.inv2rs, lp) * a.GM;
       a.gx[i] = g0;
       a.gy[i] = g1;
       a.gz[i] = g2;
@@ -598,19 +625,174 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickAr
   }
 }
 
+template <bool WRAP>
+__global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB) k_kick_pme(KickArgs a, int stage, int npass) {
+  extern __shared__ float4 smem4[];
+  int bid = blockIdx.x;
+  const int i2 = bid % a.s2;
+  bid /= a.s2;
+  const int i1 = bid % a.s1;
+  const int i0 = bid / a.s1;
+  kick_cell<WRAP>(a, a.b0 + i0, a.b1 + i1, a.b2 + i2, smem4, stage, npass);
+}
+
+// ------------------------------------------------------------ batched kick
+//
+// Many independent boxes kicked by one persistent launch.  A work item is
+// one (box, chain cell); items are ordered by estimated cost (sinks x
+// neighbourhood sources, heaviest first) and taken from a global counter,
+// so the blocks that finish light cells pick up the remaining ones and no
+// box-sized tail is left on a few SMs.  The per-box kernel arguments live in
+// a device array; the step's scalars come as kernel parameters.
+struct StepScalars {
+  int min_rung, first_call;
+  float t0, scale;
+};
+
+__device__ __forceinline__ KickArgs box_args(const KickArgs* __restrict__ boxes, int b, const StepScalars& st) {
+  KickArgs a = boxes[b];
+  a.min_rung = st.min_rung;
+  a.first_call = st.first_call;
+  a.t0 = st.t0;
+  a.scale = st.scale;
+  return a;
+}
+
+template <bool WRAP>
+__global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB)
+    k_kick_batch(const KickArgs* __restrict__ boxes, const int2* __restrict__ items, const int* __restrict__ nitems,
+                 int* __restrict__ counter, StepScalars st, int stage, int npass) {
+  extern __shared__ float4 smem4[];
+  __shared__ int s_item[2];
+  // The box's arguments are read from shared memory where they are used:
+  // held in registers, its ten array addresses would spill the pair loop.
+  __shared__ KickArgs s_args;
+  const int n = *nitems;
+  if (threadIdx.x == 0) s_item[0] = atomicAdd(counter, 1);
+  __syncthreads();
+  int cur_box = -1;
+  for (int k = 0;; k ^= 1) {
+    const int it = s_item[k];
+    if (it >= n) return;
+    // the next item is fetched while this one runs; the barrier at the end of
+    // the iteration orders the write against the reads of s_item[k ^ 1]
+    if (threadIdx.x == 0) s_item[k ^ 1] = atomicAdd(counter, 1);
+    const int2 w = __ldg(items + it);
+    if (w.x != cur_box) {  // uniform: every thread read the same item
+      if (threadIdx.x == 0) s_args = box_args(boxes, w.x, st);
+      cur_box = w.x;
+      __syncthreads();
+    }
+    const int C = s_args.C;
+    kick_cell<WRAP>(s_args, w.y % C, (w.y / C) % C, w.y / (C * C), smem4, stage, npass);
+    __syncthreads();
+  }
+}
+
+// Long-range interpolation of every item (one block per item, direct reads).
+__global__ void __launch_bounds__(64) k_interp_batch(const KickArgs* __restrict__ boxes, const int2* __restrict__ items,
+                                                      const int* __restrict__ nitems, int min_rung) {
+  if ((int)blockIdx.x >= *nitems) return;
+  const int2 w = __ldg(items + blockIdx.x);
+  interp_cell_direct(boxes[w.x], w.y, min_rung);
+}
+
+// Work items of a batch: every non-empty (box, cell), bucketed by the
+// binary order of magnitude of its cost and laid out heaviest bucket first.
+struct BoxCells {
+  const int32_t* begin;
+  int C;
+  int base;  // first global item index of the box
+};
+
+__device__ __forceinline__ int find_box(const BoxCells* __restrict__ bc, int nbox, int g) {
+  int lo = 0, hi = nbox - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&bc[mid].base) <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+constexpr int kCostClasses = 64;
+
+__device__ __forceinline__ int cell_cost_class(const BoxCells& b, int key, int& count) {
+  const int C = b.C;
+  const int cx = key % C, cy = (key / C) % C, cz = key / (C * C);
+  const int32_t n = __ldg(b.begin + key + 1) - __ldg(b.begin + key);
+  count = n;
+  if (n == 0) return -1;
+  int64_t nb = 0;
+  for (int dz = -1; dz <= 1; dz++)
+    for (int dy = -1; dy <= 1; dy++) {
+      const int64_t row = ((int64_t)wrapi(cz + dz, C) * C + wrapi(cy + dy, C)) * C;
+      for (int dx = -1; dx <= 1; dx++) {
+        const int64_t k2 = row + wrapi(cx + dx, C);
+        nb += __ldg(b.begin + k2 + 1) - __ldg(b.begin + k2);
+      }
+    }
+  const uint64_t cost = (uint64_t)n * (uint64_t)nb;
+  return 63 - __clzll((long long)(cost | 1ull));
+}
+
+__global__ void k_item_classes(const BoxCells* __restrict__ bc, int nbox, int total, int* __restrict__ cls,
+                               int* __restrict__ hist) {
+  __shared__ int sh[kCostClasses];
+  for (int i = threadIdx.x; i < kCostClasses; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < total) {
+    const int b = find_box(bc, nbox, g);
+    const BoxCells box = bc[b];
+    int cnt;
+    const int c = cell_cost_class(box, g - box.base, cnt);
+    cls[g] = c;
+    if (c >= 0) atomicAdd(&sh[c], 1);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kCostClasses; i += blockDim.x)
+    if (sh[i]) atomicAdd(hist + i, sh[i]);
+}
+
+// hist[0..63] -> start offsets, heaviest class first; nitems = total
+// non-empty items.  One warp.
+__global__ void k_item_offsets(int* __restrict__ hist, int* __restrict__ start, int* __restrict__ nitems) {
+  const int lane = threadIdx.x;
+  // lane l owns classes 63 - 2l and 62 - 2l (descending order)
+  const int a = hist[63 - 2 * lane], b = hist[62 - 2 * lane];
+  int incl = a + b;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int excl = incl - a - b;
+  start[63 - 2 * lane] = excl;
+  start[62 - 2 * lane] = excl + a;
+  if (lane == 31) *nitems = incl;
+  hist[63 - 2 * lane] = 0;  // reused as fill counters by the scatter
+  hist[62 - 2 * lane] = 0;
+}
+
+__global__ void k_item_scatter(const BoxCells* __restrict__ bc, int nbox, int total, const int* __restrict__ cls,
+                               const int* __restrict__ start, int* __restrict__ fill, int2* __restrict__ items) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int c = cls[g];
+  if (c < 0) return;
+  const int b = find_box(bc, nbox, g);
+  items[start[c] + atomicAdd(fill + c, 1)] = make_int2(b, g - __ldg(&bc[b].base));
+}
+
 }  // namespace
 
-int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0, int first_call) {
-  if (!c->sorted) return fail(TPM_ERR_STATE, "kick_pme needs chainmesh_create first");
-  if (!c->have_phi) return fail(TPM_ERR_STATE, "kick_pme needs gravity_long_compute first");
-  const int C = c->C;
-  int b[3], e[3];
-  for (int d = 0; d < 3; d++) {
-    b[d] = box ? box[d] : 0;
-    e[d] = box ? box[3 + d] : C;
-    if (b[d] < 0 || e[d] > C || e[d] < b[d]) return fail(TPM_ERR_INVALID, "kick box outside the chain mesh");
-  }
-  const int64_t ncell = (int64_t)(e[0] - b[0]) * (e[1] - b[1]) * (e[2] - b[2]);
+namespace {
+
+// Kernel arguments of one box (the reference's kernel_params,
+// src/kick_pme.cu:439-453, all FP32) for sink cells [b, e).
+KickArgs make_args(tpm_ctx* c, const int b[3], const int e[3], int min_rung, double scale, double t0,
+                   int first_call) {
   KickArgs a;
   a.pos4 = c->pos4;
   a.vx = c->vx;
@@ -625,7 +807,7 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
   a.thr = c->thr;
   a.phi = c->phi;
   a.err = c->d_err;
-  a.C = C;
+  a.C = c->C;
   a.N = c->N;
   a.b0 = b[0];
   a.b1 = b[1];
@@ -635,37 +817,63 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
   a.min_rung = min_rung;
   a.first_call = first_call ? 1 : 0;
   a.kahan = c->opt.kahan ? 1 : 0;
-  // kernel_params (src/kick_pme.cu:439-453), all FP32.
   a.GM = (float)c->opt.GM;
   a.eta = (float)c->opt.eta;
   a.t0 = (float)t0;
   a.scale = (float)scale;
   a.hsoft = (float)c->opt.hsoft;
-  const float rs = (float)c->rs_box;
-  a.inv2rs = 1.0f / rs / 2.0f;
-  a.twooversqrtpi = 2.0f / sqrtf((float)M_PI);
-  a.p_r = 0.3275911f * a.inv2rs;
-  a.e_r = -1.4426950408889634f * a.inv2rs * a.inv2rs;
-  a.c_r = a.twooversqrtpi * a.inv2rs;
-  a.h2 = a.hsoft * a.hsoft;
-  a.hinv = 1.f / a.hsoft;
-  a.h3inv = a.hinv * (a.hinv * a.hinv);
-  a.rcut2 = c->rcut_box > 0 ? (float)(c->rcut_box * c->rcut_box) : INFINITY;
-  // Block size follows the mean cell occupancy (about two groups of 8 sinks
-  // per warp, 2..8 warps); the stage holds 1.25x the mean 27-cell
-  // neighbourhood (at most kMaxStage sources; larger ones are chunked).
-  const double mean_cell = (double)c->n / ((double)C * C * C);
-  const int W = (int)std::min(8.0, std::max(2.0, std::ceil(mean_cell / (2.0 * kGroup))));
-  const int T = 32 * W;
+  const double inv2rs = 0.5 / c->rs_box;
+  a.inv2rs = (float)inv2rs;
+  a.lscale = (float)(inv2rs * 2.3283064365386963e-10);
+  a.h2 = (float)((c->opt.hsoft * inv2rs) * (c->opt.hsoft * inv2rs));
+  a.rcut2 = c->rcut_box > 0 ? (float)((c->rcut_box * inv2rs) * (c->rcut_box * inv2rs)) : INFINITY;
+  return a;
+}
+
+size_t kick_smem(const KickShape& k) {
+  return sizeof(float4) * ((size_t)k.stage + (size_t)k.warps * kBuf + k.npass) + sizeof(float) * k.npass * 8 +
+         sizeof(unsigned) * k.npass + sizeof(int) * (2 * kMaxRuns + 2);
+}
+
+}  // namespace
+
+// Block size follows the mean cell occupancy (about two groups of 8 sinks
+// per warp, 2..8 warps); the stage holds a fraction of the mean 27-cell
+// neighbourhood (at most kMaxStage sources; larger ones are chunked).
+KickShape kick_default_shape(double mean_cell) {
+  KickShape k;
+  k.warps = (int)std::min(8.0, std::max(2.0, std::ceil(mean_cell / (2.0 * kGroup))));
   int stage = (int)std::min<double>(kMaxStage, std::max<double>(512.0, TPM_KICK_STAGE_X100 * 0.01 * 27.0 * mean_cell));
-  stage = (stage + 127) / 128 * 128;
-  int npass = kPass;
+  k.stage = (stage + 127) / 128 * 128;
+  k.npass = kPass;
   if (TPM_KICK_PASS_X > 0) {
-    npass = 64;
-    while (npass < kPass && npass < TPM_KICK_PASS_X * mean_cell) npass *= 2;
+    k.npass = 64;
+    while (k.npass < kPass && k.npass < TPM_KICK_PASS_X * mean_cell) k.npass *= 2;
   }
-  const size_t smem = sizeof(float4) * ((size_t)stage + (size_t)W * kBuf + npass) + sizeof(float) * npass * 8 +
-                      sizeof(unsigned) * npass + sizeof(int) * (2 * kMaxRuns + 2);
+  return k;
+}
+
+bool kick_shape_valid(const KickShape& k) {
+  const bool pow2 = k.npass >= 8 && (k.npass & (k.npass - 1)) == 0;
+  return k.warps >= 1 && 32 * k.warps <= kKickThreads && k.stage >= 128 && k.stage <= kMaxStage &&
+         k.stage % 128 == 0 && pow2 && k.npass <= kPass && kick_smem(k) <= 200 * 1024;
+}
+
+int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0, int first_call) {
+  if (!c->sorted) return fail(TPM_ERR_STATE, "kick_pme needs chainmesh_create first");
+  if (!c->have_phi) return fail(TPM_ERR_STATE, "kick_pme needs gravity_long_compute first");
+  const int C = c->C;
+  int b[3], e[3];
+  for (int d = 0; d < 3; d++) {
+    b[d] = box ? box[d] : 0;
+    e[d] = box ? box[3 + d] : C;
+    if (b[d] < 0 || e[d] > C || e[d] < b[d]) return fail(TPM_ERR_INVALID, "kick box outside the chain mesh");
+  }
+  const int64_t ncell = (int64_t)(e[0] - b[0]) * (e[1] - b[1]) * (e[2] - b[2]);
+  const KickArgs a = make_args(c, b, e, min_rung, scale, t0, first_call);
+  const double mean_cell = (double)c->n / ((double)C * C * C);
+  const KickShape k = kick_default_shape(mean_cell);
+  const size_t smem = kick_smem(k);
   const bool wrap = C == 3;
   auto kern = wrap ? k_kick_pme<true> : k_kick_pme<false>;
   TPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -677,10 +885,9 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
   const int maxw = (c->N + C - 1) / C + 8;
   const size_t tile_bytes = sizeof(float) * (size_t)maxw * maxw * maxw;
   const double span = (double)c->N / C + 6.0;
-  const double mean_sinks = (double)c->n / ((double)C * C * C);
   stage_begin(c, kStInterp);
   if (ncell > 0) {
-    if (tile_bytes <= 48 * 1024 && span * span * span <= 16.0 * mean_sinks) {
+    if (tile_bytes <= 48 * 1024 && span * span * span <= 16.0 * mean_cell) {
       k_interp_tile<<<(unsigned)ncell, 128, tile_bytes, c->stream>>>(a, maxw);
     } else {
       k_interp_direct<<<(unsigned)ncell, 64, 0, c->stream>>>(a);
@@ -691,11 +898,79 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
   stage_end(c, kStInterp);
   stage_begin(c, kStKick);
   if (ncell > 0) {
-    kern<<<(unsigned)ncell, T, smem, c->stream>>>(a, stage, npass);
+    kern<<<(unsigned)ncell, 32 * k.warps, smem, c->stream>>>(a, k.stage, k.npass);
     c->launches++;
     TPM_CUDA_TRY(cudaGetLastError());
   }
   stage_end(c, kStKick);
+  return TPM_OK;
+}
+
+// ------------------------------------------------------------ batched kick
+
+size_t kick_batch_args_bytes() { return sizeof(KickArgs); }
+size_t kick_batch_cells_bytes() { return sizeof(BoxCells); }
+
+int kick_batch_write_tables(tpm_ctx* const* boxes, int nbox, void* h_args, void* h_cells, int64_t* total_cells) {
+  KickArgs* A = static_cast<KickArgs*>(h_args);
+  BoxCells* B = static_cast<BoxCells*>(h_cells);
+  int64_t base = 0;
+  for (int i = 0; i < nbox; i++) {
+    tpm_ctx* c = boxes[i];
+    const int b[3] = {0, 0, 0};
+    const int e[3] = {c->C, c->C, c->C};
+    A[i] = make_args(c, b, e, 0, 1.0, 1.0, 1);
+    B[i].begin = c->cell_begin;
+    B[i].C = c->C;
+    B[i].base = (int)base;
+    base += (int64_t)c->C * c->C * c->C;
+    if (base > 0x7fffffffLL) return fail(TPM_ERR_INVALID, "batch has more than 2^31 chain cells");
+  }
+  *total_cells = base;
+  return TPM_OK;
+}
+
+int kick_batch_queue(const BatchQueue& q, cudaStream_t s) {
+  if (q.total_cells <= 0) return TPM_OK;
+  const int total = (int)q.total_cells;
+  TPM_CUDA_TRY(cudaMemsetAsync(q.d_hist, 0, sizeof(int) * 2 * kCostClasses, s));
+  const unsigned blocks = (unsigned)ceil_div(total, 256);
+  k_item_classes<<<blocks, 256, 0, s>>>(static_cast<const BoxCells*>(q.d_cells), q.nbox, total, q.d_class,
+                                        q.d_hist);
+  k_item_offsets<<<1, 32, 0, s>>>(q.d_hist, q.d_hist + kCostClasses, q.d_nitems);
+  k_item_scatter<<<blocks, 256, 0, s>>>(static_cast<const BoxCells*>(q.d_cells), q.nbox, total, q.d_class,
+                                        q.d_hist + kCostClasses, q.d_hist, q.d_items);
+  TPM_CUDA_TRY(cudaGetLastError());
+  return TPM_OK;
+}
+
+int kick_batch_interp(const BatchQueue& q, int min_rung, cudaStream_t s) {
+  if (q.total_cells <= 0) return TPM_OK;
+  k_interp_batch<<<(unsigned)q.total_cells, 64, 0, s>>>(static_cast<const KickArgs*>(q.d_args), q.d_items,
+                                                         q.d_nitems, min_rung);
+  TPM_CUDA_TRY(cudaGetLastError());
+  return TPM_OK;
+}
+
+int kick_batch_kick(const BatchQueue& q, const KickShape& k, bool wrap, int min_rung, double scale, double t0,
+                    int first_call, cudaStream_t s, int* blocks_out) {
+  if (!kick_shape_valid(k)) return fail(TPM_ERR_INVALID, "invalid kick shape");
+  if (q.total_cells <= 0) return TPM_OK;
+  const size_t smem = kick_smem(k);
+  auto kern = wrap ? k_kick_batch<true> : k_kick_batch<false>;
+  TPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0, dev = 0, sms = 0;
+  TPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * k.warps, smem));
+  TPM_CUDA_TRY(cudaGetDevice(&dev));
+  TPM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (per_sm < 1) return fail(TPM_ERR_INVALID, "kick shape does not fit on an SM");
+  const int64_t blocks = std::min<int64_t>((int64_t)per_sm * sms, q.total_cells);
+  StepScalars st{min_rung, first_call ? 1 : 0, (float)t0, (float)scale};
+  TPM_CUDA_TRY(cudaMemsetAsync(q.d_counter, 0, sizeof(int), s));
+  kern<<<(unsigned)blocks, 32 * k.warps, smem, s>>>(static_cast<const KickArgs*>(q.d_args), q.d_items, q.d_nitems,
+                                                    q.d_counter, st, k.stage, k.npass);
+  TPM_CUDA_TRY(cudaGetLastError());
+  if (blocks_out) *blocks_out = (int)blocks;
   return TPM_OK;
 }
 

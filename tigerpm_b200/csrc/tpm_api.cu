@@ -20,9 +20,11 @@ int fail(int status, const std::string& msg) {
 }
 
 void stage_begin(tpm_ctx* c, Stage s) {
+  if (!c->stage_timing) return;
   cudaEventRecord(c->ev.beg[s][c->ev.count[s] % kStageSlots], c->stream);
 }
 void stage_end(tpm_ctx* c, Stage s) {
+  if (!c->stage_timing) return;
   cudaEventRecord(c->ev.end[s][c->ev.count[s] % kStageSlots], c->stream);
   c->ev.count[s]++;
 }
@@ -237,12 +239,84 @@ int tpm_plan_device_bytes(const tpm_options* opts, int64_t capacity, int64_t* by
   return TPM_OK;
 }
 
+}  // extern "C"
+
+namespace tpm {
+
+// The per-step working set of a context: everything a step writes and no
+// later call reads back (forces, packed positions, sort scratch, meshes).
+// A served box keeps only its resident set and borrows these for a step.
+namespace {
+struct ScratchField {
+  void** ptr;
+  size_t elem;
+  int64_t count;
+};
+
+std::vector<ScratchField> scratch_fields(tpm_ctx* c) {
+  const int64_t cap = std::max<int64_t>(c->cap, 1);
+  const int64_t N = c->N, C = c->C, ncell = C * C * C;
+  const int64_t nb = (std::max(cap, ncell) + kScanTileElems - 1) / kScanTileElems;
+  return {
+      {(void**)&c->gx, 4, cap},      {(void**)&c->gy, 4, cap},       {(void**)&c->gz, 4, cap},
+      {(void**)&c->pot, 4, cap},     {(void**)&c->pos4, 16, cap},    {(void**)&c->x2, 4, cap},
+      {(void**)&c->y2, 4, cap},      {(void**)&c->z2, 4, cap},       {(void**)&c->vx2, 4, cap},
+      {(void**)&c->vy2, 4, cap},     {(void**)&c->vz2, 4, cap},      {(void**)&c->rung2, 1, cap},
+      {(void**)&c->key, 4, cap},     {(void**)&c->idx, 4, cap},      {(void**)&c->cellof, 4, cap},
+      {(void**)&c->prefix, 4, cap + 1}, {(void**)&c->slot, 4, cap},  {(void**)&c->blocksum, 4, 2 * nb + 64},
+      {(void**)&c->rho, 4, N * N * N}, {(void**)&c->rhok, 8, N * N * fft3d_padded_columns((int)N)},
+      {(void**)&c->phi, 4, N * N * N},
+  };
+}
+constexpr size_t kScratchAlign = 256;
+}  // namespace
+
+int64_t ctx_scratch_bytes(tpm_ctx* c) {
+  int64_t b = 0;
+  for (const ScratchField& f : scratch_fields(c))
+    b += (int64_t)((f.elem * f.count + kScratchAlign - 1) / kScratchAlign * kScratchAlign);
+  return b;
+}
+
+void ctx_bind_scratch(tpm_ctx* c, void* base, cudaStream_t s) {
+  unsigned char* p = static_cast<unsigned char*>(base);
+  for (const ScratchField& f : scratch_fields(c)) {
+    *f.ptr = p;
+    p += (f.elem * f.count + kScratchAlign - 1) / kScratchAlign * kScratchAlign;
+  }
+  c->stream = s;
+  if (c->plans) {
+    cufftSetStream(c->plan_r2c, s);
+    cufftSetStream(c->plan_c2r, s);
+  }
+}
+
+void ctx_unbind_scratch(tpm_ctx* c, cudaStream_t own) {
+  for (const ScratchField& f : scratch_fields(c)) *f.ptr = nullptr;
+  c->stream = own;
+  if (c->plans) {
+    cufftSetStream(c->plan_r2c, own);
+    cufftSetStream(c->plan_c2r, own);
+  }
+}
+
+}  // namespace tpm
+
+extern "C" {
+
 int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out) {
+  return tpm::ctx_create(opts, capacity, true, out);
+}
+
+}  // extern "C"
+
+int tpm::ctx_create(const tpm_options* opts, int64_t capacity, bool with_scratch, tpm_ctx** out) {
   if (!opts || !out) return fail(TPM_ERR_INVALID, "null argument");
   *out = nullptr;
   if (capacity < 0 || capacity > 0x7fffffffLL - 1) return fail(TPM_ERR_INVALID, "capacity out of range");
   tpm_ctx* c = new tpm_ctx();
   c->opt = *opts;
+  c->has_scratch = with_scratch;
   int rc = derive(c);
   if (rc) {
     delete c;
@@ -265,6 +339,7 @@ int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out) {
   const int64_t N = c->N, C = c->C, ncell = C * C * C;
   const int64_t nb = (std::max(capacity, ncell) + kScanTileElems - 1) / kScanTileElems;
   Alloc A{c};
+  // resident set: particles, chain-mesh tables, FFT and Green tables
   A.get(c->x, capacity);
   A.get(c->y, capacity);
   A.get(c->z, capacity);
@@ -272,37 +347,30 @@ int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out) {
   A.get(c->vy, capacity);
   A.get(c->vz, capacity);
   A.get(c->rung, capacity);
-  A.get(c->gx, capacity);
-  A.get(c->gy, capacity);
-  A.get(c->gz, capacity);
-  A.get(c->pot, capacity);
-  A.get(c->pos4, capacity);
-  A.get(c->x2, capacity);
-  A.get(c->y2, capacity);
-  A.get(c->z2, capacity);
-  A.get(c->vx2, capacity);
-  A.get(c->vy2, capacity);
-  A.get(c->vz2, capacity);
-  A.get(c->rung2, capacity);
-  A.get(c->key, capacity);
-  A.get(c->idx, capacity);
-  A.get(c->cellof, capacity);
-  A.get(c->prefix, capacity + 1);
-  A.get(c->slot, capacity);
-  A.get(c->blocksum, 2 * nb + 64);
   A.get(c->scan_status, nb + 1);
   A.get(c->cell_count, ncell + 1);
   A.get(c->cell_begin, ncell + 1);
   A.get(c->thr, C + 1);
   A.get(c->tree, C * kMaxTreeDepth);
   A.get(c->depth1d, C);
-  A.get(c->rho, N * N * N);
-  A.get(c->rhok, N * N * fft3d_padded_columns((int)N));
   A.get(c->fft_tw, N);
-  A.get(c->phi, N * N * N);
   A.get(c->gtab, 2 * N);
   A.get(c->k2tab, N);
   A.get(c->d_err, 1);
+  // per-step working set
+  if (with_scratch) {
+    for (const auto& f : scratch_fields(c)) {
+      if (A.status != TPM_OK) break;
+      cudaError_t ea = cudaMalloc(f.ptr, f.elem * (size_t)std::max<int64_t>(f.count, 1));
+      if (ea != cudaSuccess) {
+        *f.ptr = nullptr;
+        cudaGetLastError();
+        A.status = fail(TPM_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(ea));
+      } else {
+        c->device_bytes += (int64_t)(f.elem * (size_t)std::max<int64_t>(f.count, 1));
+      }
+    }
+  }
   if (A.status != TPM_OK) {
     tpm_ctx_destroy(c);
     return A.status;
@@ -324,15 +392,19 @@ int tpm_ctx_create(const tpm_options* opts, int64_t capacity, tpm_ctx** out) {
   return TPM_OK;
 }
 
+extern "C" {
+
 int tpm_ctx_destroy(tpm_ctx* c) {
   if (!c) return TPM_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->x, c->y, c->z, c->vx, c->vy, c->vz, c->rung, c->gx, c->gy, c->gz, c->pot, c->pos4,
-                  c->x2, c->y2, c->z2, c->vx2, c->vy2, c->vz2, c->rung2, c->key, c->idx, c->cellof,
-                  c->prefix, c->slot, c->blocksum, c->scan_status, c->cell_count, c->cell_begin, c->thr, c->tree,
-                  c->depth1d, c->rho, c->rhok, c->fft_tw, c->phi, c->gtab, c->k2tab, c->d_err};
+  void* ptrs[] = {c->x, c->y, c->z, c->vx, c->vy, c->vz, c->rung, c->scan_status, c->cell_count, c->cell_begin,
+                  c->thr, c->tree, c->depth1d, c->fft_tw, c->gtab, c->k2tab, c->d_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  // a borrowed working set (served boxes) belongs to its lender
+  if (c->has_scratch)
+    for (const auto& f : scratch_fields(c))
+      if (*f.ptr) cudaFree(*f.ptr);
   if (c->plans) {
     cufftDestroy(c->plan_r2c);
     cufftDestroy(c->plan_c2r);
@@ -422,6 +494,7 @@ int tpm_get_particles(tpm_ctx* c, uint32_t* x, uint32_t* y, uint32_t* z, float* 
 
 int tpm_get_forces(tpm_ctx* c, float* gx, float* gy, float* gz, float* pot) {
   if (!c) return fail(TPM_ERR_INVALID, "null context");
+  if (!c->gx) return fail(TPM_ERR_STATE, "no forces: a served box keeps no working set between steps");
   const int64_t n = c->n;
   cudaStream_t s = c->stream;
   if (n > 0) {

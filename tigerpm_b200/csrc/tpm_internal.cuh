@@ -124,6 +124,16 @@ struct tpm_ctx {
   cudaEvent_t ev_up[3] = {}, ev_done[3] = {}, ev_down[3] = {};
   bool pipe_ready = false;
 
+  // Batch members: the sort copies its result back into x..rung instead of
+  // swapping buffers, so device addresses stay fixed across steps (captured
+  // CUDA graphs and per-box kernel-argument tables keep them); stage events
+  // are skipped (a batch times its own phases).
+  bool stable_buffers = false;
+  bool stage_timing = true;
+  // false: the per-step working set (forces, pos4, sort scratch, meshes) is
+  // not owned; a server binds one for each step (ctx_bind_scratch)
+  bool has_scratch = true;
+
   int* d_err = nullptr;
   int64_t launches = 0;
   int64_t device_bytes = 0;
@@ -136,6 +146,41 @@ namespace tpm {
 // Stage timing helpers.
 void stage_begin(tpm_ctx* c, Stage s);
 void stage_end(tpm_ctx* c, Stage s);
+
+// Launch shape of the kick kernel: warps per block, sources staged per
+// chunk, sinks per pass.
+struct KickShape {
+  int warps, stage, npass;
+};
+KickShape kick_default_shape(double mean_cell);
+bool kick_shape_valid(const KickShape& k);
+
+// Work queue of a batched kick over many boxes (device arrays).
+struct BatchQueue {
+  int nbox = 0;
+  int64_t total_cells = 0;   // sum of the boxes' chain cells
+  void* d_args = nullptr;    // per-box kernel arguments (kick_batch_args_bytes each)
+  void* d_cells = nullptr;   // per-box cell tables (kick_batch_cells_bytes each)
+  int* d_class = nullptr;    // cost class of every (box, cell), total_cells
+  int* d_hist = nullptr;     // 2 x 64 ints
+  int2* d_items = nullptr;   // (box, cell key), heaviest first, total_cells
+  int* d_nitems = nullptr;   // non-empty items
+  int* d_counter = nullptr;  // persistent-kernel work counter
+};
+size_t kick_batch_args_bytes();
+size_t kick_batch_cells_bytes();
+int kick_batch_write_tables(tpm_ctx* const* boxes, int nbox, void* h_args, void* h_cells, int64_t* total_cells);
+int kick_batch_queue(const BatchQueue& q, cudaStream_t s);
+int kick_batch_interp(const BatchQueue& q, int min_rung, cudaStream_t s);
+int kick_batch_kick(const BatchQueue& q, const KickShape& k, bool wrap, int min_rung, double scale, double t0,
+                    int first_call, cudaStream_t s, int* blocks_out);
+
+// Contexts with or without their per-step working set; the set's size and
+// binding (the lender keeps the memory; own = the stream to return to).
+int ctx_create(const tpm_options* opts, int64_t capacity, bool with_scratch, tpm_ctx** out);
+int64_t ctx_scratch_bytes(tpm_ctx* c);
+void ctx_bind_scratch(tpm_ctx* c, void* base, cudaStream_t s);
+void ctx_unbind_scratch(tpm_ctx* c, cudaStream_t own);
 
 // Kernel families (each returns TPM_OK or an error).
 int chainmesh_sort(tpm_ctx* c);

@@ -152,3 +152,38 @@ def log_uniform_sides(count: int, lo: int, hi: int, seed: int) -> np.ndarray:
     """Box sides n = round(exp(U[ln lo, ln hi])) for the batched / served pools."""
     g = rng(seed)
     return np.rint(np.exp(g.uniform(math.log(lo), math.log(hi), count))).astype(np.int64)
+
+
+def fft_friendly(n_min: int) -> int:
+    """Smallest mesh side >= n_min that the library's own FFT takes: a
+    multiple of 16 whose cofactor has no prime factor above 5."""
+    m = max(16, (int(n_min) + 15) // 16 * 16)
+    while True:
+        k = m // 16
+        for p in (2, 3, 5):
+            while k % p == 0:
+                k //= p
+        if k == 1:
+            return m
+        m += 16
+
+
+def accurate_box_params(n_side: int) -> dict:
+    """Mesh and split parameters of a box of n_side^3 particles in the form
+    that meets rms force error <= 1e-4 against FP64 Ewald: the reference's
+    cloud4 deposit on a mesh of at least 3 points per particle spacing
+    (rounded up to a size the library's FFT takes), split scale r_s = 2/3
+    particle spacing and cutoff 6 r_s = 4 particle spacings (64 particles
+    per chain cell on average)."""
+    grid = fft_friendly(3 * n_side)
+    rs_cells = 2.0 * grid / (3.0 * n_side)
+    return dict(n_side=n_side, grid=grid, rs_cells=rs_cells, rcut_over_rs=6.0, assign="cloud4")
+
+
+def ensemble(count: int, lo: int, hi: int, seed: int, rms_cells: float = 0.3):
+    """The batched / served pools: `count` Zel'dovich boxes (P(k) ~ k^-2 cut
+    at k_Nyq/2, rms displacement rms_cells particle spacings) with sides
+    log-uniform in [lo, hi] and per-box seeds.  Returns (sides, [ParticleSet])."""
+    sides = log_uniform_sides(count, lo, hi, seed)
+    sets = [zeldovich(int(n), seed * 1000 + i + 1, rms_cells=rms_cells, grid=int(n)) for i, n in enumerate(sides)]
+    return sides, sets
