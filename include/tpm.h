@@ -318,6 +318,41 @@ int tpm_pme_steps_host(tpm_ctx* ctx, int64_t nsteps, int64_t n, const tpm_host_p
  * step beyond 2^31 box lengths. */
 int tpm_check_errors(tpm_ctx* ctx);
 
+/* -------------------------------------------------- initial conditions
+ *
+ * Zel'dovich initial conditions generated on the device (initialize and
+ * zeldovich_begin / zeldovich_end, src/initialize.cpp:91-221): one complex
+ * normal deviate per mode times sqrt(P(k)) K / k^2, the kz = 0 plane made
+ * Hermitian (fft3d_force_real, src/fft.cpp:86-123), an inverse FFT, and
+ * x = (I + 1/2) / N + displacement, wrapped, as fixed32.  Deviates come from
+ * Philox-4x32-10 keyed by `seed` with the mode's array indices as counter
+ * (the reference draws GSL taus sequentially).
+ *   npower > 0: P(k) is the reference's table form (power.init columns k in
+ *     h/Mpc and P in (Mpc/h)^3; cubic interpolation in ln k, normalised to
+ *     the context's sigma8; amplitude from its code_to_cm box size and the
+ *     growth factor at z0), unless rms_disp > 0 rescales it;
+ *   npower = 0: P(k) = k^index exp(-k / (kcut_over_nyq k_Nyq)) in mode
+ *     units, scaled to an rms displacement of rms_disp particle spacings.
+ * Writes n_side^3 particles (x-major lattice order, zero velocities and
+ * rungs) into the context; dxmax = the largest |displacement| in spacings. */
+typedef struct tpm_ic_params {
+  int n_side;
+  uint64_t seed;
+  int npower;
+  const double* power_k;
+  const double* power_p;
+  double index;
+  double kcut_over_nyq;
+  double rms_disp;
+} tpm_ic_params;
+int tpm_ic_zeldovich(tpm_ctx* ctx, const tpm_ic_params* params, double* dxmax);
+/* The power_spectrum_function of a table (src/initialize.cpp:10-66,182-211)
+ * evaluated at nk wavenumbers (1/Mpc), normalised to sigma8. */
+int tpm_ic_power(const double* table_k, const double* table_p, int npower, double hubble, double sigma8, int nk,
+                 const double* k, double* p_out);
+/* growth_factor (src/initialize.cpp:76-83). */
+int tpm_growth_factor(double omega_m, double a, double* out);
+
 /* ------------------------------------------------------------ batches
  *
  * An ensemble of independent periodic boxes (each with its own particle

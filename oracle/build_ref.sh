@@ -29,6 +29,12 @@ extract "$REF/src/particles.cpp" '^int particles_sort\(int begin, int end, doubl
 extract "$REF/src/chainmesh.cpp" '^static void sort\(const range<int> chain_box, int pbegin, int pend\) \{' "$TMP/chainmesh_sort.inc"
 extract "$REF/src/gravity_long.cpp" '^double cloud4\(double x\)' "$TMP/cloud4.inc"
 extract "$REF/src/gravity_long.cpp" '^void apply_laplacian\(gravity_long_type type\)' "$TMP/apply_laplacian.inc"
+# initial conditions: the power-spectrum table, its sigma8 normalisation and
+# the growth factor (src/initialize.cpp:10-66,76-83,182-211)
+awk '/^struct power_spectrum_function \{/ {f = 1} f == 1 {print} f == 1 && /^};/ {exit}' "$REF/src/initialize.cpp" > "$TMP/power_spectrum.inc"
+[ -s "$TMP/power_spectrum.inc" ] || { echo "could not extract power_spectrum_function" >&2; exit 1; }
+extract "$REF/src/initialize.cpp" '^double growth_factor\(double omega_m, float a\)' "$TMP/growth_factor.inc"
+extract "$REF/src/initialize.cpp" '^static power_spectrum_function read_power_spectrum\(\) \{' "$TMP/read_power_spectrum.inc"
 
 # nvcc (host code) so that tigerpm/tigerpm.hpp skips its HPX include
 ARCH="-gencode arch=compute_100a,code=sm_100a"

@@ -276,3 +276,66 @@ def drift(p: Particles, dt: float) -> None:
 
 def max_threads() -> int:
     return int(lib().orc_max_threads())
+
+
+# ------------------------------------------------------- initial conditions
+
+def philox4x32_10(ctr, key):
+    """Philox-4x32-10 (Salmon et al. SC'11) of one 4-word counter, 2-word key."""
+    c = np.ascontiguousarray(ctr, np.uint32)
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.empty(4, np.uint32)
+    L = lib()
+    L.orc_philox4x32_10.argtypes = [u32p, u32p, u32p]
+    L.orc_philox4x32_10(c, k, out)
+    return out
+
+
+def ic_power(table_k, table_p, hubble: float, sigma8: float, k):
+    """power_spectrum_function (src/initialize.cpp:10-66,182-211) at k (1/Mpc)."""
+    tk = np.ascontiguousarray(table_k, np.float64)
+    tp = np.ascontiguousarray(table_p, np.float64)
+    k = np.ascontiguousarray(k, np.float64)
+    out = np.empty(k.size)
+    L = lib()
+    L.orc_ic_power.restype = C.c_int
+    L.orc_ic_power.argtypes = [f64p, f64p, C.c_int, C.c_double, C.c_double, C.c_int64, f64p, f64p]
+    if L.orc_ic_power(tk, tp, tk.size, hubble, sigma8, k.size, k, out):
+        raise ValueError("orc_ic_power failed")
+    return out
+
+
+def growth_factor(omega_m: float, a: float) -> float:
+    """growth_factor (src/initialize.cpp:76-83)."""
+    L = lib()
+    L.orc_growth_factor.restype = C.c_double
+    L.orc_growth_factor.argtypes = [C.c_double, C.c_double]
+    return float(L.orc_growth_factor(omega_m, a))
+
+
+def ic_zeldovich(N: int, seed: int, table_k=None, table_p=None, index: float = -2.0, kcut: float = 0.5,
+                 rms_disp: float = 0.0, hubble: float = 0.7, sigma8: float = 0.84, code_to_cm: float = 0.0,
+                 omega_m: float = 0.3, z0: float = 2.0):
+    """zeldovich_begin / fft3d_force_real / zeldovich_end (src/initialize.cpp:91-180)
+    in FP64 with Philox deviates; returns (x, y, z) fixed32 and max |dx| N."""
+    n = N ** 3
+    x = np.empty(n, np.uint32)
+    y = np.empty(n, np.uint32)
+    z = np.empty(n, np.uint32)
+    dmax = C.c_double()
+    if table_k is None:
+        tk = tp = np.zeros(1)
+        npow = 0
+    else:
+        tk = np.ascontiguousarray(table_k, np.float64)
+        tp = np.ascontiguousarray(table_p, np.float64)
+        npow = tk.size
+    L = lib()
+    L.orc_ic_zeldovich.restype = C.c_int
+    L.orc_ic_zeldovich.argtypes = [C.c_int, C.c_uint64, C.c_int, f64p, f64p, C.c_double, C.c_double, C.c_double,
+                                   C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, u32p, u32p, u32p,
+                                   C.POINTER(C.c_double)]
+    if L.orc_ic_zeldovich(N, seed, npow, tk, tp, index, kcut, rms_disp, hubble, sigma8, code_to_cm, omega_m, z0,
+                          x, y, z, C.byref(dmax)):
+        raise ValueError("orc_ic_zeldovich failed")
+    return x, y, z, float(dmax.value)

@@ -118,6 +118,14 @@ struct apply_laplacian_action {};
 #include "cloud4.inc"
 #include "apply_laplacian.inc"
 
+// initial conditions (src/initialize.cpp): the reader opens "power.init" in
+// the working directory
+#include <cmath>
+#include <limits>
+#include "power_spectrum.inc"
+#include "growth_factor.inc"
+#include "read_power_spectrum.inc"
+
 static std::vector<char> slurp(const char* path) {
   FILE* f = fopen(path, "rb");
   if (!f) {
@@ -212,6 +220,26 @@ int main(int argc, char** argv) {
     apply_laplacian(type);
     FILE* f = fopen(argv[6], "wb");
     fwrite(g_Y.data(), 8, cnt, f);
+    fclose(f);
+    return 0;
+  }
+  if (mode == "power" && argc == 6) {
+    // power <hubble> <sigma8> <in> <out>; power.init in the working directory
+    // in: m, k[m] (f64, 1/Mpc), then q, (omega_m, a)[q] (f64)
+    // out: P(k)[m] (f32 as f64), growth_factor[q] (f64)
+    g_opts.hubble = atof(argv[2]);
+    g_opts.sigma8 = atof(argv[3]);
+    const auto in = slurp(argv[4]);
+    const int64_t m = *(const int64_t*)in.data();
+    const double* k = (const double*)(in.data() + 8);
+    const int64_t q = *(const int64_t*)(in.data() + 8 + 8 * m);
+    const double* oa = (const double*)(in.data() + 16 + 8 * m);
+    const power_spectrum_function func = read_power_spectrum();
+    std::vector<double> out(m + q);
+    for (int64_t i = 0; i < m; i++) out[i] = func((float)k[i]);
+    for (int64_t i = 0; i < q; i++) out[m + i] = growth_factor(oa[2 * i], (float)oa[2 * i + 1]);
+    FILE* f = fopen(argv[5], "wb");
+    fwrite(out.data(), 8, m + q, f);
     fclose(f);
     return 0;
   }

@@ -96,3 +96,23 @@ def ewald(x, y, z, sx, sy, sz, hsoft):
     out = _run("ref_gpu", ["ewald", None, None], pay)
     v = np.frombuffer(out, "<f8").reshape(4, ns).copy()
     return v[0], v[1], v[2], v[3]
+
+
+def power(table_k, table_p, hubble: float, sigma8: float, k, omega_a):
+    """read_power_spectrum + power_spectrum_function + growth_factor
+    (src/initialize.cpp:10-83,182-211) on a power.init written from the
+    given table (k in h/Mpc, P in (Mpc/h)^3).  Returns (P(k), growth)."""
+    k = np.ascontiguousarray(k, np.float64)
+    oa = np.ascontiguousarray(omega_a, np.float64).reshape(-1, 2)
+    pay = (struct.pack("<q", k.size) + k.tobytes() + struct.pack("<q", oa.shape[0]) + oa.tobytes())
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "power.init"), "w") as f:
+            for a, b in zip(table_k, table_p):
+                f.write(f"   {a:.5E}   {b:.5E}\n")
+        fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(pay)
+        subprocess.run([os.path.join(REF, "ref_cpu"), "power", repr(hubble), repr(sigma8), fin, fout], check=True,
+                       stdout=subprocess.DEVNULL, cwd=d)
+        out = np.fromfile(fout, np.float64)
+    return out[:k.size], out[k.size:]

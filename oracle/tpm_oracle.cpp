@@ -999,3 +999,183 @@ int orc_drift(int64_t n, uint32_t* x, uint32_t* y, uint32_t* z, const float* vx,
 int orc_max_threads() { return omp_get_max_threads(); }
 
 }  // extern "C"
+
+// ------------------------------------------------------ initial conditions
+
+namespace {
+
+// Philox-4x32-10 (Salmon, Moraes, Dror & Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11): ten rounds; each multiplies counter words 0 and 2
+// by the round multipliers, swaps and xors the high halves with the other
+// words and the key, and bumps the key by the Weyl constants.
+void philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; r++) {
+    const uint64_t a = (uint64_t)0xD2511F53u * c[0];
+    const uint64_t b = (uint64_t)0xCD9E8D57u * c[2];
+    const uint32_t n0 = (uint32_t)(b >> 32) ^ c[1] ^ k0;
+    const uint32_t n1 = (uint32_t)b;
+    const uint32_t n2 = (uint32_t)(a >> 32) ^ c[3] ^ k1;
+    const uint32_t n3 = (uint32_t)a;
+    c[0] = n0;
+    c[1] = n1;
+    c[2] = n2;
+    c[3] = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+// power_spectrum_function (src/initialize.cpp:10-66) in double, with the
+// table transformation of read_power_spectrum (:182-211).
+struct Spectrum {
+  std::vector<double> P;
+  double lo = 0, hi = 0, step = 1;
+  double eval(double k) const {
+    const double t = (std::log(k) - lo) / step;
+    int i0 = std::min(std::max((int)t - 1, 0), (int)P.size() - 4);
+    const double x = t - (i0 + 1);
+    double y[4];
+    for (int q = 0; q < 4; q++) y[q] = std::log(P[i0 + q]);
+    const double s1 = 0.5 * (y[2] - y[0]), s2 = 0.5 * (y[3] - y[1]);
+    // cubic Hermite between y1 and y2 with central-difference slopes
+    const double c2 = -2 * s1 - s2 - 3 * y[1] + 3 * y[2];
+    const double c3 = s1 + s2 + 2 * y[1] - 2 * y[2];
+    return std::exp(y[1] + x * (s1 + x * (c2 + x * c3)));
+  }
+  double w8(double lnk, double h) const {  // sigma8 integrand over ln k
+    const double R = 8.0 / h, k = std::exp(lnk);
+    const double u = std::sin(k * R) - k * R * std::cos(k * R);
+    return 9.0 / (2.0 * M_PI * M_PI) / std::pow(R, 6) * eval(k) * u * u / (k * k * k);
+  }
+  int build(const double* tk, const double* tp, int n, double h, double sigma8) {
+    if (n < 4) return -1;
+    P.resize(n);
+    double kmin = 1e300, kmax = 0;
+    for (int i = 0; i < n; i++) {
+      P[i] = tp[i] / (h * h * h);
+      kmin = std::min(kmin, tk[i] * h);
+      kmax = std::max(kmax, tk[i] * h);
+    }
+    lo = std::log(kmin);
+    hi = std::log(kmax);
+    step = (hi - lo) / (n - 1);
+    const int m = 8192;  // Simpson's rule
+    const double d = (hi - lo) / m;
+    double s = (w8(lo, h) + w8(hi, h)) * d / 3.0;
+    for (int i = 1; i < m; i++) s += (i % 2 ? 4.0 : 2.0) / 3.0 * w8(lo + i * d, h) * d;
+    for (double& p : P) p *= sigma8 * sigma8 / s;
+    return 0;
+  }
+};
+
+// growth_factor (src/initialize.cpp:76-83), a taken in single precision and
+// the literals 4/7 and 1/70 as the reference's float constants.
+double growth(double om, double a_in) {
+  const double a = (double)(float)a_in;
+  const double ol = 1.0 - om, a3 = a * a * a;
+  const double Om = om / (om + a3 * ol), Ol = a3 * ol / (om + a3 * ol);
+  return 2.5 * a * Om / (std::pow(Om, (double)(4.f / 7.f)) - Ol + (1 + Om / 2) * (1 + (double)0.014285714f * Ol));
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_philox4x32_10(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+  philox(c, key[0], key[1]);
+  for (int i = 0; i < 4; i++) out[i] = c[i];
+}
+
+int orc_ic_power(const double* tk, const double* tp, int n, double h, double sigma8, int64_t nk, const double* k,
+                 double* out) {
+  Spectrum s;
+  if (s.build(tk, tp, n, h, sigma8)) return -1;
+  for (int64_t i = 0; i < nk; i++) out[i] = s.eval(k[i]);
+  return 0;
+}
+
+double orc_growth_factor(double om, double a) { return growth(om, a); }
+
+// zeldovich_begin / fft3d_force_real / zeldovich_end (src/initialize.cpp:91-180,
+// src/fft.cpp:86-123) in FP64 with the library's deviates: Philox-4x32-10 keyed
+// by seed, counter = (i, j, kz, 0) of the half-spectrum element; x = (u0 + 1)
+// 2^-32, y = u1 2^-32, deviate exp(2 pi i y) sqrt(-ln x).  npower > 0: table
+// spectrum (k in h/Mpc) with the physical amplitude L^-1.5 N^3 and -D1/L
+// (L = code_to_cm / 3.086e24 Mpc); npower = 0: k^index exp(-k / (kcut k_Nyq))
+// in mode units.  rms_disp > 0 rescales the displacement to that rms in
+// particle spacings.  Positions in lattice order (x-major), fixed32.
+int orc_ic_zeldovich(int N, uint64_t seed, int npower, const double* tk, const double* tp, double index,
+                     double kcut, double rms_disp, double h, double sigma8, double code_to_cm, double omega_m,
+                     double z0, uint32_t* x, uint32_t* y, uint32_t* z, double* dxmax) {
+  const int Nh = N / 2 + 1;
+  const int64_t m_end = (int64_t)N * N / 4;
+  std::vector<double> amp(std::max<int64_t>(m_end, 1), 0.0);
+  double kunit = 1.0, L = 1.0, scale = -1.0;
+  if (npower > 0) {
+    Spectrum s;
+    if (s.build(tk, tp, npower, h, sigma8)) return -1;
+    L = code_to_cm / 3.086e24;
+    kunit = 2.0 * M_PI / L;
+    const double f = std::pow(L, -1.5) * (double)N * N * N;
+    for (int64_t m = 1; m < m_end; m++) {
+      const double k = kunit * std::sqrt((double)m);
+      amp[m] = std::sqrt(s.eval(k)) * f / (k * k);
+    }
+    scale = -(growth(omega_m, 1.0 / (z0 + 1.0)) / growth(omega_m, 1.0)) / L;
+  } else {
+    if (!(kcut > 0) || !(rms_disp > 0)) return -1;
+    for (int64_t m = 1; m < m_end; m++) {
+      const double k = std::sqrt((double)m);
+      amp[m] = std::sqrt(std::pow(k, index) * std::exp(-k / (kcut * 0.5 * N))) / (k * k);
+    }
+  }
+  auto smode = [N](int i) { return i < N / 2 ? i : i - N; };
+  auto value = [&](int i, int j, int kz, int d) -> cd {
+    const int a = smode(i), b = smode(j), c = smode(kz);
+    const int64_t i2 = (int64_t)a * a + (int64_t)b * b + (int64_t)c * c;
+    if (i2 <= 0 || i2 >= m_end) return cd(0, 0);
+    uint32_t ctr[4] = {(uint32_t)i, (uint32_t)j, (uint32_t)kz, 0u};
+    philox(ctr, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const double u = ((double)ctr[0] + 1.0) / kTwo32, v = (double)ctr[1] / kTwo32;
+    const double r = std::sqrt(-std::log(u));
+    const int K[3] = {a, b, c};
+    const double A = amp[i2] * kunit * K[d];
+    return cd(r * std::cos(2 * M_PI * v) * A, r * std::sin(2 * M_PI * v) * A);
+  };
+  const int64_t n = (int64_t)N * N * N;
+  std::vector<std::vector<double>> disp(3, std::vector<double>(n));
+  std::vector<cd> Y((size_t)N * N * Nh);
+  for (int d = 0; d < 3; d++) {
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < (int64_t)N * N * Nh; e++) {
+      const int kz = (int)(e % Nh), j = (int)((e / Nh) % N), i = (int)(e / ((int64_t)N * Nh));
+      cd v = value(i, j, kz, d);
+      if (kz == 0) v = 0.5 * (v + std::conj(value((N - i) % N, (N - j) % N, 0, d)));
+      Y[e] = v;
+    }
+    fft3d_c2r(N, Y.data(), disp[d].data());  // carries 1/N^3 as the reference's inverse
+  }
+  if (rms_disp > 0) {
+    double ss = 0;
+    for (int d = 0; d < 3; d++)
+      for (int64_t p = 0; p < n; p++) ss += disp[d][p] * disp[d][p];
+    scale = -(rms_disp / N) / std::sqrt(ss / (double)n);
+  }
+  uint32_t* X[3] = {x, y, z};
+  double mx = 0;
+  for (int64_t p = 0; p < n; p++) {
+    const int I[3] = {(int)(p / ((int64_t)N * N)), (int)((p / N) % N), (int)(p % N)};
+    for (int d = 0; d < 3; d++) {
+      const double dx = scale * disp[d][p];
+      mx = std::max(mx, std::fabs(dx * N));
+      double q = (I[d] + 0.5) / N + dx;
+      q -= std::floor(q);
+      X[d][p] = (uint32_t)std::min(q * kTwo32, 4294967295.0);
+    }
+  }
+  if (dxmax) *dxmax = mx;
+  return 0;
+}
+
+}  // extern "C"

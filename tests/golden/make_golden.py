@@ -122,6 +122,22 @@ def make_cpu(out):
             res[f"out{typ}"] = R.laplacian(N, rs_cells, typ, Y)
         np.savez_compressed(os.path.join(out, f"laplacian_N{N}.npz"), N=np.int32(N),
                             rs_cells=np.float64(rs_cells), Y=Y, **res)
+    # initial conditions: the reference's power-table reader, log-cubic
+    # interpolation, sigma8 normalisation and growth factor, run on a table of
+    # our own (P ~ k T(k)^2 with the BBKS transfer function, Bardeen et al.
+    # 1986, Gamma = 0.21), written in power.init's format
+    tk = np.logspace(-4, 2, 300)
+    q = tk / 0.21
+    T = np.log1p(2.34 * q) / (2.34 * q) * (1 + 3.89 * q + (16.1 * q) ** 2 + (5.46 * q) ** 3 + (6.71 * q) ** 4) ** -0.25
+    tp = 2.0e4 * tk * T ** 2
+    tk = np.array([float(f"{v:.5E}") for v in tk])
+    tp = np.array([float(f"{v:.5E}") for v in tp])
+    hubble, sigma8 = 0.7, 0.84
+    ks = np.concatenate([np.logspace(-4.6, 2.3, 400) * hubble, 2 * np.pi / 100.0 * np.sqrt(np.arange(1, 200))])
+    oa = np.array([[0.3, 1 / 3], [0.3, 0.5], [0.3, 1.0], [0.25, 0.1], [1.0, 0.5], [0.3, 1 / 1.5]])
+    pk, gf = R.power(tk, tp, hubble, sigma8, ks, oa)
+    np.savez_compressed(os.path.join(out, "ic_power.npz"), table_k=tk, table_p=tp, hubble=np.float64(hubble),
+                        sigma8=np.float64(sigma8), k=ks, P=pk, omega_a=oa, growth=gf)
 
 
 def kick_inputs():

@@ -82,6 +82,13 @@ class ServeStats(C.Structure):
                 ("steps_done", C.c_int64), ("particles_done", C.c_int64), ("launches", C.c_int64)]
 
 
+class ICParams(C.Structure):
+    """struct tpm_ic_params."""
+    _fields_ = [("n_side", C.c_int), ("seed", C.c_uint64), ("npower", C.c_int), ("power_k", C.c_void_p),
+                ("power_p", C.c_void_p), ("index", C.c_double), ("kcut_over_nyq", C.c_double),
+                ("rms_disp", C.c_double)]
+
+
 BATCH_RESTORE = 1
 BATCH_GRAPH = 2
 
@@ -150,6 +157,9 @@ SIGNATURES = [
     ("tpm_batch_get_shape", _I, [_P, C.POINTER(KickShape)]),
     ("tpm_batch_set_shape", _I, [_P, C.POINTER(KickShape)]),
     ("tpm_batch_autotune", _I, [_P, _I, _I, C.POINTER(KickShape)]),
+    ("tpm_ic_zeldovich", _I, [_P, C.POINTER(ICParams), C.POINTER(_D)]),
+    ("tpm_ic_power", _I, [_P, _P, _I, _D, _D, _I, _P, _P]),
+    ("tpm_growth_factor", _I, [_D, _D, C.POINTER(_D)]),
     ("tpm_serve_create", _I, [_I64, _I, C.POINTER(_P)]),
     ("tpm_serve_destroy", _I, [_P]),
     ("tpm_serve_add_box", _I, [_P, C.POINTER(Options), _I64, _P, _P, _P, _P, _P, _P, _P, C.POINTER(_I)]),

@@ -375,6 +375,34 @@ class TigerPM:
         return int(a.value), int(b.value)
 
 
+def ic_zeldovich(ctx: "TigerPM", n_side: int, seed: int, table_k=None, table_p=None, index: float = -2.0,
+                 kcut_over_nyq: float = 0.5, rms_disp: float = 0.0) -> float:
+    """Zel'dovich initial conditions generated on the device into ctx
+    (tpm_ic_zeldovich): a power.init-style table (k h/Mpc, P (Mpc/h)^3) with
+    the reference's sigma8 / growth-factor amplitude, or (no table)
+    P ~ k^index exp(-k / (kcut_over_nyq k_Nyq)); rms_disp > 0 rescales to
+    that rms displacement in particle spacings.  Returns max |dx| in spacings."""
+    lib = _lib.load()
+    p = _lib.ICParams()
+    p.n_side = int(n_side)
+    p.seed = int(seed)
+    keep = []
+    if table_k is not None:
+        tk = np.ascontiguousarray(table_k, np.float64)
+        tp = np.ascontiguousarray(table_p, np.float64)
+        keep += [tk, tp]
+        p.npower = tk.size
+        p.power_k = tk.ctypes.data
+        p.power_p = tp.ctypes.data
+    p.index = float(index)
+    p.kcut_over_nyq = float(kcut_over_nyq)
+    p.rms_disp = float(rms_disp)
+    dmax = C.c_double()
+    check(lib.tpm_ic_zeldovich(ctx.h, C.byref(p), C.byref(dmax)), "ic_zeldovich")
+    ctx.n = int(n_side) ** 3
+    return float(dmax.value)
+
+
 class Batch:
     """An ensemble of independent periodic boxes kicked together
     (tpm_batch_*): every box's sort and long-range solve run concurrently,
