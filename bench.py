@@ -376,6 +376,74 @@ def batch_arm(args, rank, world, dist, n_boxes=64, lo=32, hi=128):
             "speedup_vs_sequential": round(ms_seq / ms, 3), "accuracy": acc}
 
 
+def serve_arm(args, rank, world, dist, pool=256, lo=32, hi=192, rate=200.0, seconds=12.0, slots=8):
+    """Config 5: a resident pool of `pool` Zel'dovich boxes (sides
+    log-uniform in [lo, hi], generated on the device, each on its own mesh),
+    kick + drift requests arriving as a Poisson process at `rate` per second
+    for `seconds`, admitted by the HBM budget into up to `slots` concurrent
+    steps.  Latency = submission to completion (host clock)."""
+    from tigerpm_b200 import workloads as W
+    from tigerpm_b200.api import Server, TigerPM, ic_zeldovich
+    g = W.rng(args.seed + 90 + rank)
+    sides = W.log_uniform_sides(pool, lo, hi, args.seed + 70 + rank)
+    opts = ensemble_opts(sides)
+    t_gen = time.perf_counter()
+    srv = Server(budget_bytes=0, max_slots=slots)
+    ids = [srv.add_box_ic(o, int(n), seed=args.seed * 1000 + 7 * i + 3) for i, (o, n) in enumerate(zip(opts, sides))]
+    t_gen = time.perf_counter() - t_gen
+    dt = 1e-4
+    # warm-up: every slot and the working-set pool see a few steps
+    warm = [srv.submit(ids[int(j)], dt) for j in g.integers(0, pool, 4 * slots)]
+    for r in warm:
+        srv.wait(r)
+    nreq = int(rate * seconds)
+    arrivals = np.cumsum(g.exponential(1.0 / rate, nreq))
+    which = g.integers(0, pool, nreq)
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    res = srv.replay([ids[int(j)] for j in which], arrivals, dt)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    lat = np.array([r["latency_ms"] for r in res])
+    qms = np.array([r["queue_ms"] for r in res])
+    dev = np.array([r["device_ms"] for r in res])
+    parts = float(sum(r["particles"] for r in res))
+    srv.close()
+    # accuracy of the served step form: the same step (sort + PME + kick) on
+    # two pool boxes through a context, against FP64 Ewald
+    acc = None
+    if args.ewald_samples:
+        num = den = 0.0
+        cnt = 0
+        for j in (int(np.argmin(np.abs(sides - np.median(sides)))), int(np.argmax(sides))):
+            n = int(sides[j])
+            with TigerPM(opts[j], n ** 3) as t:
+                ic_zeldovich(t, n, args.seed * 1000 + 7 * j + 3, rms_disp=0.3)
+                t.pme_step(0, 1.0, 1.0, True)
+                idx = W.sample_indices(n ** 3, 512, args.seed + j)
+                gx, gy, gz, _ = t.get_forces()
+                _, gref = t.ewald_samples(idx, 1)
+                gk = np.stack([gx[idx], gy[idx], gz[idx]], 1).astype(np.float64)
+                num += float(np.sum((gk - gref) ** 2))
+                den += float(np.sum(gref * gref))
+                cnt += idx.size
+        acc = {"force_rms_vector": float(f"{math.sqrt(num / den):.4e}"), "samples": cnt, "boxes": 2}
+    return {"config": f"{pool} resident Zel'dovich boxes, sides log-uniform in [{lo}, {hi}] (seeded, generated on "
+                      f"the device), each on its own cloud4 mesh >= 3 points per spacing; kick + drift requests, "
+                      f"Poisson arrivals at {rate:g}/s for {seconds:g} s; up to {slots} steps in flight",
+            "requests": nreq, "particles_pool": int(sum(int(n) ** 3 for n in sides)),
+            "value": parts / wall, "unit": "particle-kicks/s",
+            "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3),
+                           "mean": round(float(lat.mean()), 3), "max": round(float(lat.max()), 3)},
+            "queue_ms": {"p50": round(float(np.percentile(qms, 50)), 3), "p99": round(float(np.percentile(qms, 99)), 3)},
+            "device_ms": {"p50": round(float(np.percentile(dev, 50)), 3), "p99": round(float(np.percentile(dev, 99)), 3)},
+            "wall_s": round(wall, 3), "offered_s": round(float(arrivals[-1]), 3),
+            "device_busy_frac_sum": round(float(dev.sum() / 1e3 / wall), 3),
+            "stats": st, "generation_s": round(t_gen, 2), "accuracy": acc,
+            "api": "tpm_serve_replay (submit at arrival, dispatcher admits by HBM budget)"}
+
+
 def read_traffic(name):
     """DRAM bytes per kick launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", f"kick_pme_{name}.md")
@@ -438,6 +506,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-named", action="store_true", help="skip the literal c2 secondary measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble secondary measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream secondary measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -488,6 +557,9 @@ def main():
     batch = None
     if args.config == "c2-accurate" and not args.no_batch:
         batch = batch_arm(args, rank, world, dist)
+    serve = None
+    if args.config == "c2-accurate" and not args.no_serve:
+        serve = serve_arm(args, rank, world, dist)
     named = {}
     if args.config == "c2-accurate" and not args.no_named:
         # the configurations' literal forms, measured in the same run: the
@@ -506,6 +578,8 @@ def main():
         if batch is not None:
             batch["vs_plain_single_box"] = round(batch["value"] / res["value"], 4)
             line["batch"] = batch
+        if serve is not None:
+            line["serve"] = serve
         for nm, r in named.items():
             entry = {"config": workload_desc(nm, CONFIGS[nm], make_opts(CONFIGS[nm])),
                      "value": r["value"], "ms_per_step": r["ms_per_step"], "e2e": r["e2e"]["value"],

@@ -318,6 +318,44 @@ int tpm_pme_steps_host(tpm_ctx* ctx, int64_t nsteps, int64_t n, const tpm_host_p
  * step beyond 2^31 box lengths. */
 int tpm_check_errors(tpm_ctx* ctx);
 
+/* ------------------------------------------------------- integration
+ *
+ * Rung-based kick-drift-kick over one big step t0.  The reference supplies
+ * the kick of a block time-step scheme (kick_pme with min_rung and
+ * first_call, src/kick_pme.cu:319-354) but no driver and no drift.  Time runs
+ * on integer ticks, 2^31 per t0; a particle on rung r is kicked every
+ * t0 / 2^r.  tpm_integrate_begin (first_call = 1) kicks every particle
+ * (opening half-kicks, rungs assigned).  Each substep finds the largest rung
+ * R, drifts every particle to the next multiple of 2^(31-R) ticks and kicks
+ * the particles due there, min_rung = 31 - ctz(tick) (every particle at the
+ * end of the big step).  Each kick is chainmesh_create +
+ * gravity_long_compute(PME) + kick_pme. */
+typedef struct tpm_substep {
+  int64_t tick;           /* ticks of t0 / ticks_per_step reached by the substep */
+  int64_t ticks_per_step; /* 2^31 */
+  int max_rung;           /* largest rung before the substep */
+  int min_rung;           /* particles kicked: rung >= min_rung */
+  double drift_dt;        /* time the substep drifted */
+  int done;               /* 1 at the end of the big step */
+} tpm_substep;
+
+int tpm_integrate_begin(tpm_ctx* ctx, double t0, double scale, int first_call);
+int tpm_integrate_substep(tpm_ctx* ctx, tpm_substep* info);
+/* The whole big step; log (optional) receives up to log_cap substeps. */
+int tpm_integrate(tpm_ctx* ctx, double t0, double scale, int first_call, int max_substeps, tpm_substep* log,
+                  int log_cap, int* nsub);
+
+/* FP64 reductions over the particles, per particle (equal masses): kinetic
+ * energy <v^2 / 2>, potential energy <phi / 2> (NaN unless the last kick
+ * covered every particle since the last sort or drift) and momentum <v>. */
+typedef struct tpm_diag {
+  double kinetic;
+  double potential;
+  double momentum[3];
+  int64_t n;
+} tpm_diag;
+int tpm_diagnostics(tpm_ctx* ctx, tpm_diag* out);
+
 /* -------------------------------------------------- initial conditions
  *
  * Zel'dovich initial conditions generated on the device (initialize and
@@ -468,6 +506,9 @@ int tpm_serve_destroy(tpm_server* s);
 int tpm_serve_add_box(tpm_server* s, const tpm_options* opts, int64_t n, const uint32_t* x, const uint32_t* y,
                       const uint32_t* z, const float* vx, const float* vy, const float* vz, const int8_t* rung,
                       int* box_id);
+/* The same with the box's particles generated on the device by
+ * tpm_ic_zeldovich (n = n_side^3). */
+int tpm_serve_add_box_ic(tpm_server* s, const tpm_options* opts, const tpm_ic_params* ic, int* box_id);
 /* Queues one step of a box (tpm_pme_step arguments + drift dt); returns at once. */
 int tpm_serve_submit(tpm_server* s, int box, double dt, int min_rung, double scale, double t0, int first_call,
                      int* req_id);

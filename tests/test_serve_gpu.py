@@ -114,6 +114,23 @@ def test_budget_admission_and_errors():
             s.submit(99, DT)
 
 
+def test_box_admitted_with_device_ic():
+    """A box admitted with on-device initial conditions holds exactly what
+    tpm_ic_zeldovich writes into a plain context."""
+    from tigerpm_b200.api import ic_zeldovich
+    n = 20
+    p = W.accurate_box_params(n)
+    o = make_options(n, p["grid"], rs_cells=p["rs_cells"], rcut_over_rs=p["rcut_over_rs"], assign="cloud4")
+    with Server(max_slots=2) as s:
+        b = s.add_box_ic(o, n, seed=77, rms_disp=0.3)
+        got = s.box(b).get_particles()
+        s.wait(s.submit(b, DT))
+    with TigerPM(o, n ** 3) as t:
+        ic_zeldovich(t, n, 77, rms_disp=0.3)
+        ref = t.get_particles()
+    _same(got, ref)
+
+
 def test_poisson_replay_latencies():
     boxes = [_box(n, 80 + n, deterministic=False) for n in (16, 24, 32, 20)]
     g = W.rng(9)

@@ -82,6 +82,18 @@ class ServeStats(C.Structure):
                 ("steps_done", C.c_int64), ("particles_done", C.c_int64), ("launches", C.c_int64)]
 
 
+class Substep(C.Structure):
+    """struct tpm_substep."""
+    _fields_ = [("tick", C.c_int64), ("ticks_per_step", C.c_int64), ("max_rung", C.c_int), ("min_rung", C.c_int),
+                ("drift_dt", C.c_double), ("done", C.c_int)]
+
+
+class Diag(C.Structure):
+    """struct tpm_diag."""
+    _fields_ = [("kinetic", C.c_double), ("potential", C.c_double), ("momentum", C.c_double * 3),
+                ("n", C.c_int64)]
+
+
 class ICParams(C.Structure):
     """struct tpm_ic_params."""
     _fields_ = [("n_side", C.c_int), ("seed", C.c_uint64), ("npower", C.c_int), ("power_k", C.c_void_p),
@@ -157,12 +169,17 @@ SIGNATURES = [
     ("tpm_batch_get_shape", _I, [_P, C.POINTER(KickShape)]),
     ("tpm_batch_set_shape", _I, [_P, C.POINTER(KickShape)]),
     ("tpm_batch_autotune", _I, [_P, _I, _I, C.POINTER(KickShape)]),
+    ("tpm_integrate_begin", _I, [_P, _D, _D, _I]),
+    ("tpm_integrate_substep", _I, [_P, C.POINTER(Substep)]),
+    ("tpm_integrate", _I, [_P, _D, _D, _I, _I, _P, _I, C.POINTER(_I)]),
+    ("tpm_diagnostics", _I, [_P, C.POINTER(Diag)]),
     ("tpm_ic_zeldovich", _I, [_P, C.POINTER(ICParams), C.POINTER(_D)]),
     ("tpm_ic_power", _I, [_P, _P, _I, _D, _D, _I, _P, _P]),
     ("tpm_growth_factor", _I, [_D, _D, C.POINTER(_D)]),
     ("tpm_serve_create", _I, [_I64, _I, C.POINTER(_P)]),
     ("tpm_serve_destroy", _I, [_P]),
     ("tpm_serve_add_box", _I, [_P, C.POINTER(Options), _I64, _P, _P, _P, _P, _P, _P, _P, C.POINTER(_I)]),
+    ("tpm_serve_add_box_ic", _I, [_P, C.POINTER(Options), C.POINTER(ICParams), C.POINTER(_I)]),
     ("tpm_serve_submit", _I, [_P, _I, _D, _I, _D, _D, _I, C.POINTER(_I)]),
     ("tpm_serve_wait", _I, [_P, _I, C.POINTER(ServeResult)]),
     ("tpm_serve_drain", _I, [_P]),

@@ -278,6 +278,30 @@ class TigerPM:
     def drift(self, dt: float) -> None:
         check(self.lib.tpm_drift(self.h, float(dt)), "drift")
 
+    # ------------------------------------------------------- integration
+    def integrate_begin(self, t0: float, scale: float = 1.0, first_call: bool = True) -> None:
+        check(self.lib.tpm_integrate_begin(self.h, float(t0), float(scale), 1 if first_call else 0),
+              "integrate_begin")
+
+    def integrate_substep(self) -> dict:
+        s = _lib.Substep()
+        check(self.lib.tpm_integrate_substep(self.h, C.byref(s)), "integrate_substep")
+        return {n: getattr(s, n) for n, _ in _lib.Substep._fields_}
+
+    def integrate(self, t0: float, scale: float = 1.0, first_call: bool = True, max_substeps: int = 1 << 12):
+        """One big step of rung-based kick-drift-kick; returns the substeps."""
+        log = (_lib.Substep * max_substeps)()
+        k = C.c_int()
+        check(self.lib.tpm_integrate(self.h, float(t0), float(scale), 1 if first_call else 0, int(max_substeps),
+                                     log, int(max_substeps), C.byref(k)), "integrate")
+        return [{n: getattr(log[i], n) for n, _ in _lib.Substep._fields_} for i in range(k.value)]
+
+    def diagnostics(self) -> dict:
+        """FP64 per-particle kinetic and potential energy and momentum."""
+        d = _lib.Diag()
+        check(self.lib.tpm_diagnostics(self.h, C.byref(d)), "diagnostics")
+        return {"kinetic": d.kinetic, "potential": d.potential, "momentum": list(d.momentum), "n": d.n}
+
     # ---------------------------------------------------------------- Ewald
     def gravity_short_ewald_call_kernel(self, sinkx, sinky, sinkz, method: int = 1):
         """FP64 Ewald at the sink positions from all particles of the box:
@@ -536,6 +560,23 @@ class Server:
                                          _ptr(vy), _ptr(vz), _ptr(r), C.byref(bid)), "serve_add_box")
         self.opts.append(opts)
         self.counts.append(int(x.size))
+        return int(bid.value)
+
+    def add_box_ic(self, opts: Options, n_side: int, seed: int, rms_disp: float = 0.3, index: float = -2.0,
+                   kcut_over_nyq: float = 0.5) -> int:
+        """Admits a box whose Zel'dovich particles are generated on the device
+        (P ~ k^index exp(-k / (kcut k_Nyq)), rms displacement rms_disp spacings)."""
+        p = _lib.ICParams()
+        p.n_side = int(n_side)
+        p.seed = int(seed)
+        p.npower = 0
+        p.index = float(index)
+        p.kcut_over_nyq = float(kcut_over_nyq)
+        p.rms_disp = float(rms_disp)
+        bid = C.c_int()
+        check(self.lib.tpm_serve_add_box_ic(self.h, C.byref(opts), C.byref(p), C.byref(bid)), "serve_add_box_ic")
+        self.opts.append(opts)
+        self.counts.append(int(n_side) ** 3)
         return int(bid.value)
 
     def submit(self, box: int, dt: float, min_rung: int = 0, scale: float = 1.0, t0: float = 1.0,

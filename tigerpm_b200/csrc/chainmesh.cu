@@ -584,6 +584,7 @@ int chainmesh_sort(tpm_ctx* c) {
   }
   stage_end(c, kStSort);
   c->sorted = true;
+  c->pot_valid = false;  // forces and potentials are not permuted with the particles
   c->host_cells_valid = false;
   return TPM_OK;
 }

@@ -45,6 +45,7 @@ int drift(tpm_ctx* c, double dt) {
   // positions moved: the chain mesh, packed positions and potential are stale
   c->sorted = false;
   c->have_phi = false;
+  c->pot_valid = false;
   c->host_cells_valid = false;
   return TPM_OK;
 }

@@ -903,6 +903,7 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
     TPM_CUDA_TRY(cudaGetLastError());
   }
   stage_end(c, kStKick);
+  c->pot_valid = min_rung <= 0 && ncell == (int64_t)C * C * C;
   return TPM_OK;
 }
 

@@ -243,6 +243,10 @@ void dispatcher(tpm_server* s) {
   }
 }
 
+// Admits a box whose particles `init` writes into its new context.
+template <class Init>
+int add_box(tpm_server* s, const tpm_options* opts, int64_t n, Init init, int* box_id);
+
 }  // namespace
 
 extern "C" {
@@ -319,6 +323,24 @@ int tpm_serve_add_box(tpm_server* s, const tpm_options* opts, int64_t n, const u
                       const uint32_t* z, const float* vx, const float* vy, const float* vz, const int8_t* rung,
                       int* box_id) {
   if (!s || !opts || !box_id) return fail(TPM_ERR_INVALID, "null argument");
+  return add_box(s, opts, n, [&](tpm_ctx* c) { return tpm_set_particles(c, n, x, y, z, vx, vy, vz, rung); },
+                 box_id);
+}
+
+// The same with the box's particles generated on the device
+// (tpm_ic_zeldovich) instead of copied from the host.
+int tpm_serve_add_box_ic(tpm_server* s, const tpm_options* opts, const tpm_ic_params* ic, int* box_id) {
+  if (!s || !opts || !ic || !box_id) return fail(TPM_ERR_INVALID, "null argument");
+  const int64_t n = (int64_t)ic->n_side * ic->n_side * ic->n_side;
+  return add_box(s, opts, n, [&](tpm_ctx* c) { return tpm_ic_zeldovich(c, ic, nullptr); }, box_id);
+}
+
+}  // extern "C"
+
+namespace {
+
+template <class Init>
+int add_box(tpm_server* s, const tpm_options* opts, int64_t n, Init init, int* box_id) {
   tpm_ctx* c = nullptr;
   // plan first: resident and working-set bytes without allocating
   {
@@ -342,7 +364,7 @@ int tpm_serve_add_box(tpm_server* s, const tpm_options* opts, int64_t n, const u
   if (rc) return rc;
   c->stable_buffers = true;
   c->stage_timing = false;
-  rc = tpm_set_particles(c, n, x, y, z, vx, vy, vz, rung);
+  rc = init(c);
   if (rc == TPM_OK) rc = cudaStreamSynchronize(c->stream) == cudaSuccess ? TPM_OK : fail(TPM_ERR_CUDA, "sync");
   if (rc) {
     tpm_ctx_destroy(c);
@@ -364,6 +386,10 @@ int tpm_serve_add_box(tpm_server* s, const tpm_options* opts, int64_t n, const u
   *box_id = (int)s->boxes.size() - 1;
   return TPM_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 // Queues one kick + drift step of a box; returns at once with its id.
 int tpm_serve_submit(tpm_server* s, int box, double dt, int min_rung, double scale, double t0, int first_call,

@@ -133,6 +133,13 @@ struct tpm_ctx {
   // false: the per-step working set (forces, pos4, sort scratch, meshes) is
   // not owned; a server binds one for each step (ctx_bind_scratch)
   bool has_scratch = true;
+  // pot holds every particle's potential in the current order (a kick of
+  // the whole box with min_rung 0 since the last sort)
+  bool pot_valid = false;
+  // big-step integrator state (integrate.cu): ticks of t0 / 2^31
+  double int_t0 = 0, int_scale = 1;
+  int64_t int_tick = 0;
+  bool int_active = false;
 
   int* d_err = nullptr;
   int64_t launches = 0;
