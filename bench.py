@@ -444,6 +444,63 @@ def serve_arm(args, rank, world, dist, pool=256, lo=32, hi=192, rate=200.0, seco
             "api": "tpm_serve_replay (submit at arrival, dispatcher admits by HBM budget)"}
 
 
+def clustered_arm(args, rank, world, dist, n_side=256, steps=2):
+    """Config 3 form: 70 % of the particles in 2,000 NFW halos (masses
+    log-uniform over 3 decades, c in [5, 15]), 30 % uniform; the accurate
+    mesh form (cloud4, mesh 3x the lattice, r_s = 2 cells, cutoff 6 r_s).
+    The step with the default persistent (cell, sink pass) queue and with the
+    per-cell launch, and the error against FP64 Ewald."""
+    import torch
+    from tigerpm_b200 import workloads as W
+    from tigerpm_b200.api import TigerPM
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    t_gen = time.perf_counter()
+    ps = W.nfw_halos(n_side, args.seed + 30 + rank, n_halo=2000, halo_frac=0.7)
+    t_gen = time.perf_counter() - t_gen
+    opts = ensemble_opts([n_side])[0]
+    out = {"config": f"{n_side}^3 particles, 70% in 2000 NFW halos (c 5-15, masses log-uniform over 3 decades), "
+                     f"30% uniform; {opts.four_dim}^3 cloud4 mesh, r_s = 2 cells, cutoff 6 r_s, chain mesh "
+                     f"{opts.chain_dim}^3", "particles": ps.n, "generation_s": round(t_gen, 1)}
+    for mode in (0, 1):
+        opts.kick_grid = mode
+        with TigerPM(opts, ps.n) as t:
+            ext = torch.cuda.ExternalStream(t.stream(), device=dev)
+            t.set_particles(ps)
+            t.pme_step(0, 1.0, 1.0, True)
+            t.synchronize()
+            if mode == 0:
+                offs = t.chainmesh_offsets()
+                cnt = np.diff(offs)
+                out["occupancy"] = {"max": int(cnt.max()), "mean": float(cnt.mean()),
+                                    "max_over_mean": round(float(cnt.max() / cnt.mean()), 1)}
+            t.reset_stage_times()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            for _ in range(steps):
+                t.set_particles(ps)
+                t.pme_step(0, 1.0, 1.0, True)
+            e1.record(ext)
+            e1.synchronize()
+            ms = max_over_ranks(e0.elapsed_time(e1), dist, dev) / steps
+            st = t.stage_times()
+            key = "queue" if mode == 0 else "per_cell_launch"
+            out[key] = {"ms_per_step": round(ms, 3), "value": ps.n * world / (ms * 1e-3),
+                        "kick_ms": round(st["kick_ms"], 3), "interp_ms": round(st["interp_ms"], 3),
+                        "sort_ms": round(st["sort_ms"], 3)}
+            if mode == 0:
+                cand, inside = t.count_pairs(0)
+                out["pairs_in_cutoff"] = inside
+                out["pairs_candidate"] = cand
+                if args.ewald_samples:
+                    t.check_errors()
+                    err = t.gravity_short_ewald_compare(1024, seed=args.seed + 9)
+                    out["accuracy"] = {k: (float(f"{v:.4e}") if isinstance(v, float) else v) for k, v in err.items()}
+    out["value"] = out["queue"]["value"]
+    out["speedup_queue_vs_per_cell"] = round(out["per_cell_launch"]["ms_per_step"] / out["queue"]["ms_per_step"], 3)
+    return out
+
+
 def read_traffic(name):
     """DRAM bytes per kick launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", f"kick_pme_{name}.md")
@@ -507,6 +564,9 @@ def main():
     ap.add_argument("--no-named", action="store_true", help="skip the literal c2 secondary measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble secondary measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream secondary measurement")
+    ap.add_argument("--no-clustered", action="store_true", help="skip the NFW-halo secondary measurement")
+    ap.add_argument("--clustered-side", type=int, default=256,
+                    help="particles per side of the NFW-halo box (512 = the full configuration)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -560,6 +620,9 @@ def main():
     serve = None
     if args.config == "c2-accurate" and not args.no_serve:
         serve = serve_arm(args, rank, world, dist)
+    clustered = None
+    if args.config == "c2-accurate" and not args.no_clustered:
+        clustered = clustered_arm(args, rank, world, dist, n_side=args.clustered_side)
     named = {}
     if args.config == "c2-accurate" and not args.no_named:
         # the configurations' literal forms, measured in the same run: the
@@ -580,6 +643,8 @@ def main():
             line["batch"] = batch
         if serve is not None:
             line["serve"] = serve
+        if clustered is not None:
+            line["named_config_c3"] = clustered
         for nm, r in named.items():
             entry = {"config": workload_desc(nm, CONFIGS[nm], make_opts(CONFIGS[nm])),
                      "value": r["value"], "ms_per_step": r["ms_per_step"], "e2e": r["e2e"]["value"],

@@ -103,6 +103,9 @@ typedef struct tpm_options {
                               * 0: FP32 shared-memory atomics (default, faster) */
   int fft;             /* TPM_FFT_*: 3-D transforms of gravity_long_compute */
   uint64_t seed;       /* synthetic-input seed carried for drivers */
+  int kick_grid;       /* 0: the PP + kick as one persistent launch over a cost-sorted
+                        * queue of (cell, sink pass) items (default; balances clustered
+                        * boxes); 1: one block per sink cell */
 } tpm_options;
 
 typedef struct tpm_ctx tpm_ctx;

@@ -119,8 +119,14 @@ int restore(tpm_batch* b, int i) {
   return TPM_OK;
 }
 
+// Phase timing events: under stream capture they must be external records
+// (graph nodes that record on every replay); outside it, plain records.
 void record(tpm_batch* b, int k) {
-  if (b->timed) cudaEventRecordWithFlags(b->ev_t[k], b->stream, cudaEventRecordExternal);
+  if (!b->timed) return;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(b->stream, &st);
+  if (st == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(b->ev_t[k], b->stream, cudaEventRecordExternal);
+  else cudaEventRecord(b->ev_t[k], b->stream);
 }
 
 // One whole batch step on b->stream (also used under stream capture).
@@ -139,10 +145,10 @@ int issue_step(tpm_batch* b, int flags, int min_rung, double scale, double t0, i
     TPM_CUDA_TRY(cudaStreamWaitEvent(b->stream, b->ev_join[i], 0));
   }
   record(b, 1);
-  int rc = kick_batch_queue(b->q, b->stream);
+  int rc = kick_batch_queue(b->q, b->shape.npass, b->stream);
   if (rc) return rc;
   record(b, 2);
-  rc = kick_batch_interp(b->q, min_rung, b->stream);
+  rc = kick_batch_interp(b->q, min_rung, b->shape.npass, b->stream);
   if (rc) return rc;
   record(b, 3);
   rc = kick_batch_kick(b->q, b->shape, b->wrap, min_rung, scale, t0, first_call, b->stream, nullptr);
@@ -224,7 +230,8 @@ int tpm_batch_create(int nbox, const tpm_options* opts, const int64_t* capacity,
   b->mean_cell = cells > 0 ? parts / cells : 0;
   // per-box kernel arguments and cell tables (device addresses are fixed)
   std::vector<unsigned char> h_args(kick_batch_args_bytes() * nbox), h_cells(kick_batch_cells_bytes() * nbox);
-  int rc = kick_batch_write_tables(b->box.data(), nbox, h_args.data(), h_cells.data(), &b->q.total_cells);
+  int rc = kick_batch_write_tables(b->box.data(), nbox, h_args.data(), h_cells.data(), &b->q.total_cells,
+                                   &b->q.max_items);
   if (rc) return bail(rc);
   b->q.nbox = nbox;
   const int64_t T = std::max<int64_t>(b->q.total_cells, 1);
@@ -232,7 +239,7 @@ int tpm_batch_create(int nbox, const tpm_options* opts, const int64_t* capacity,
   if (e == cudaSuccess) e = cudaMalloc(&b->q.d_cells, h_cells.size());
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->q.d_class, sizeof(int) * T);
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->q.d_hist, sizeof(int) * 128);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&b->q.d_items, sizeof(int2) * T);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->q.d_items, sizeof(int4) * std::max<int64_t>(b->q.max_items, 1));
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->q.d_nitems, sizeof(int) * 2);
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->q.d_counter, sizeof(int) * 2);
   if (e == cudaSuccess) e = cudaMemcpy(b->q.d_args, h_args.data(), h_args.size(), cudaMemcpyHostToDevice);
@@ -459,7 +466,7 @@ int tpm_batch_autotune(tpm_batch* b, int min_rung, int repeats, tpm_kick_shape* 
   };
   int rc = save(false);
   if (rc) return rc;
-  rc = kick_batch_queue(b->q, s);
+  rc = TPM_OK;  // the queue depends on the pass size: built per candidate
   if (rc) return rc;
   std::vector<KickShape> cand;
   const double m = std::max(b->mean_cell, 1.0);
@@ -484,7 +491,8 @@ int tpm_batch_autotune(tpm_batch* b, int min_rung, int repeats, tpm_kick_shape* 
     float tot = 0;
     for (int r = 0; r < repeats && rc == TPM_OK; r++) {
       rc = save(true);
-      if (rc == TPM_OK) rc = kick_batch_interp(b->q, min_rung, s);
+      if (rc == TPM_OK) rc = kick_batch_queue(b->q, k.npass, s);
+      if (rc == TPM_OK) rc = kick_batch_interp(b->q, min_rung, k.npass, s);
       if (rc == TPM_OK && cudaEventRecord(e0, s) != cudaSuccess) rc = fail(TPM_ERR_CUDA, "event");
       if (rc == TPM_OK) rc = kick_batch_kick(b->q, k, b->wrap, min_rung, 1.0, 1.0, 1, s, nullptr);
       if (rc == TPM_OK && cudaEventRecord(e1, s) != cudaSuccess) rc = fail(TPM_ERR_CUDA, "event");

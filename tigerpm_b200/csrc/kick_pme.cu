@@ -125,6 +125,11 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
     iy[k] = wrapi(base[1] + k, N) * N;
     iz[k] = wrapi(base[2] + k, N);
   }
+  // The sums run over phi minus its value at the stencil's centre point:
+  // the derivative weights sum to zero, so the gradient is a difference of
+  // nearly equal terms, and removing the common value keeps FP32 from
+  // cancelling it away (the weights sum to one, so phi adds it back).
+  const float pc = __ldg(a.phi + (int64_t)wrapi(base[0] + 2, N) * N * N + iy[2] + iz[2]);
   float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
   for (int i = 0; i < kNInterp; i++) {
     const int64_t plane = (int64_t)wrapi(base[0] + i, N) * N * N;
@@ -134,7 +139,7 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
       float rz = 0.f, rdz = 0.f;
 #pragma unroll
       for (int k = 0; k < kNInterp; k++) {
-        const float v = __ldg(a.phi + plane + iy[j] + iz[k]);
+        const float v = __ldg(a.phi + plane + iy[j] + iz[k]) - pc;
         rz = fmaf(w[2][k], v, rz);
         rdz = fmaf(dw[2][k], v, rdz);
       }
@@ -150,7 +155,7 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
   lx = -sx * (float)N;
   ly = -sy * (float)N;
   lz = -sz * (float)N;
-  lp = sp;
+  lp = sp + pc;
 }
 
 // Long-range part at every active sink of the kick box, stored in gx/gy/gz/pot
@@ -202,6 +207,8 @@ __device__ __forceinline__ void interp_tile(const float* __restrict__ tile, int 
   const int ox = min(max(base[0] - bx, 0), W0 - kNInterp);
   const int oy = min(max(base[1] - by, 0), W1 - kNInterp);
   const int oz = min(max(base[2] - bz, 0), W2 - kNInterp);
+  // sums over phi minus the stencil's centre value, as in interp_long
+  const float pc = tile[(ox + 2) * W1 * W2 + (oy + 2) * W2 + oz + 2];
   float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
   for (int i = 0; i < kNInterp; i++) {
     const float* plane = tile + (ox + i) * W1 * W2 + oy * W2 + oz;
@@ -211,7 +218,7 @@ __device__ __forceinline__ void interp_tile(const float* __restrict__ tile, int 
       float rz = 0.f, rdz = 0.f;
 #pragma unroll
       for (int k = 0; k < kNInterp; k++) {
-        const float v = plane[j * W2 + k];
+        const float v = plane[j * W2 + k] - pc;
         rz = fmaf(w[2][k], v, rz);
         rdz = fmaf(dw[2][k], v, rdz);
       }
@@ -227,7 +234,7 @@ __device__ __forceinline__ void interp_tile(const float* __restrict__ tile, int 
   lx = -sx * (float)N;
   ly = -sy * (float)N;
   lz = -sz * (float)N;
-  lp = sp;
+  lp = sp + pc;
 }
 
 __global__ void __launch_bounds__(128) k_interp_tile(KickArgs a, int maxw) {
@@ -382,11 +389,14 @@ constexpr int kGroup = 8;
 constexpr int kBuf = 64;
 constexpr int kMaxRuns = 18;
 
-// The whole kick of one sink cell (cx, cy, cz) by the calling block; every
-// thread of the block calls it with the same arguments.
+// The kick of sink passes [pass_lo, pass_hi) of one sink cell (cx, cy, cz)
+// by the calling block (a pass = the cell's sinks taken np at a time, np =
+// the power of two >= the cell's count, at most npass); every thread of the
+// block calls it with the same arguments.  A pass streams the whole 27-cell
+// neighbourhood, so the passes of one cell are independent work items.
 template <bool WRAP>
 __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int cz, float4* smem4, int stage,
-                                          int npass) {
+                                          int npass, int pass_lo = 0, int pass_hi = 0x7fffffff) {
   const int T = blockDim.x, W = T >> 5;
   float4* src = smem4;
   float4* bufs = src + stage;
@@ -439,7 +449,8 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
   float4* buf = bufs + warp * kBuf;
   int np = 8;  // sinks per pass: the power of two >= the cell's count, at most npass
   while (np < npass && np < pe - pb) np <<= 1;
-  for (int32_t sbase = pb; sbase < pe; sbase += np) {
+  const int32_t s_end = (int32_t)min((int64_t)pe, (int64_t)pb + (int64_t)pass_hi * np);
+  for (int32_t sbase = pb + pass_lo * np; sbase < s_end; sbase += np) {
     // 1. order this pass's active sinks by sub-cell (deterministic bitonic sort)
     if (tid == 0) runp[kMaxRuns + 1] = np;  // active count when every slot is active
     for (int e = tid; e < np; e += T) {
@@ -660,7 +671,7 @@ __device__ __forceinline__ KickArgs box_args(const KickArgs* __restrict__ boxes,
 
 template <bool WRAP>
 __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB)
-    k_kick_batch(const KickArgs* __restrict__ boxes, const int2* __restrict__ items, const int* __restrict__ nitems,
+    k_kick_batch(const KickArgs* __restrict__ boxes, const int4* __restrict__ items, const int* __restrict__ nitems,
                  int* __restrict__ counter, StepScalars st, int stage, int npass) {
   extern __shared__ float4 smem4[];
   __shared__ int s_item[2];
@@ -677,32 +688,51 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB)
     // the next item is fetched while this one runs; the barrier at the end of
     // the iteration orders the write against the reads of s_item[k ^ 1]
     if (threadIdx.x == 0) s_item[k ^ 1] = atomicAdd(counter, 1);
-    const int2 w = __ldg(items + it);
+    const int4 w = __ldg(items + it);  // (box, cell key, first pass, end pass)
     if (w.x != cur_box) {  // uniform: every thread read the same item
       if (threadIdx.x == 0) s_args = box_args(boxes, w.x, st);
       cur_box = w.x;
       __syncthreads();
     }
     const int C = s_args.C;
-    kick_cell<WRAP>(s_args, w.y % C, (w.y / C) % C, w.y / (C * C), smem4, stage, npass);
+    kick_cell<WRAP>(s_args, w.y % C, (w.y / C) % C, w.y / (C * C), smem4, stage, npass, w.z, w.w);
     __syncthreads();
   }
 }
 
-// Long-range interpolation of every item (one block per item, direct reads).
-__global__ void __launch_bounds__(64) k_interp_batch(const KickArgs* __restrict__ boxes, const int2* __restrict__ items,
-                                                      const int* __restrict__ nitems, int min_rung) {
+// Long-range interpolation of every item's sinks (one block per item,
+// direct reads).
+__global__ void __launch_bounds__(64) k_interp_batch(const KickArgs* __restrict__ boxes, const int4* __restrict__ items,
+                                                      const int* __restrict__ nitems, int min_rung, int npass) {
   if ((int)blockIdx.x >= *nitems) return;
-  const int2 w = __ldg(items + blockIdx.x);
-  interp_cell_direct(boxes[w.x], w.y, min_rung);
+  const int4 w = __ldg(items + blockIdx.x);
+  const KickArgs& a = boxes[w.x];
+  const int32_t pb = __ldg(a.begin + w.y), pe = __ldg(a.begin + w.y + 1);
+  int np = 8;
+  while (np < npass && np < pe - pb) np <<= 1;
+  const int32_t lo = pb + w.z * np;
+  const int32_t hi = (int32_t)min((int64_t)pe, (int64_t)pb + (int64_t)w.w * np);
+  for (int32_t i = lo + (int32_t)threadIdx.x; i < hi; i += blockDim.x) {
+    if (a.rung[i] < min_rung) continue;
+    float lx, ly, lz, lp;
+    interp_long(a, __ldg(a.pos4 + i), lx, ly, lz, lp);
+    a.gx[i] = lx;
+    a.gy[i] = ly;
+    a.gz[i] = lz;
+    a.pot[i] = lp;
+  }
 }
 
-// Work items of a batch: every non-empty (box, cell), bucketed by the
+// Work items: every non-empty (box, cell) of the kick boxes, bucketed by the
 // binary order of magnitude of its cost and laid out heaviest bucket first.
+// A cell with more sinks than one pass is split into one item per pass (a
+// halo cell a thousand times the mean then spreads over many SMs).
 struct BoxCells {
   const int32_t* begin;
   int C;
-  int base;  // first global item index of the box
+  int base;    // first global cell index of the box
+  int b[3];    // kick box [b, e) in chain cells
+  int e[3];
 };
 
 __device__ __forceinline__ int find_box(const BoxCells* __restrict__ bc, int nbox, int g) {
@@ -717,11 +747,16 @@ __device__ __forceinline__ int find_box(const BoxCells* __restrict__ bc, int nbo
 
 constexpr int kCostClasses = 64;
 
-__device__ __forceinline__ int cell_cost_class(const BoxCells& b, int key, int& count) {
+// Items of one cell: none outside the kick box or when empty; one item per
+// sink pass (np = the power of two >= the cell's count, at most npass) when
+// the cell needs more than one pass, else one item for the whole cell.  All
+// of a cell's items share one cost class: sinks of a pass x neighbourhood
+// sources.  Returns class | items << 6, or -1.
+__device__ __forceinline__ int cell_items(const BoxCells& b, int key, int npass) {
   const int C = b.C;
   const int cx = key % C, cy = (key / C) % C, cz = key / (C * C);
+  if (cx < b.b[0] || cx >= b.e[0] || cy < b.b[1] || cy >= b.e[1] || cz < b.b[2] || cz >= b.e[2]) return -1;
   const int32_t n = __ldg(b.begin + key + 1) - __ldg(b.begin + key);
-  count = n;
   if (n == 0) return -1;
   int64_t nb = 0;
   for (int dz = -1; dz <= 1; dz++)
@@ -732,11 +767,14 @@ __device__ __forceinline__ int cell_cost_class(const BoxCells& b, int key, int& 
         nb += __ldg(b.begin + k2 + 1) - __ldg(b.begin + k2);
       }
     }
-  const uint64_t cost = (uint64_t)n * (uint64_t)nb;
-  return 63 - __clzll((long long)(cost | 1ull));
+  int np = 8;
+  while (np < npass && np < n) np <<= 1;
+  const int passes = (n + np - 1) / np;
+  const uint64_t cost = (uint64_t)min(n, np) * (uint64_t)nb;
+  return (63 - __clzll((long long)(cost | 1ull))) | (passes << 6);
 }
 
-__global__ void k_item_classes(const BoxCells* __restrict__ bc, int nbox, int total, int* __restrict__ cls,
+__global__ void k_item_classes(const BoxCells* __restrict__ bc, int nbox, int total, int npass, int* __restrict__ cls,
                                int* __restrict__ hist) {
   __shared__ int sh[kCostClasses];
   for (int i = threadIdx.x; i < kCostClasses; i += blockDim.x) sh[i] = 0;
@@ -745,18 +783,17 @@ __global__ void k_item_classes(const BoxCells* __restrict__ bc, int nbox, int to
   if (g < total) {
     const int b = find_box(bc, nbox, g);
     const BoxCells box = bc[b];
-    int cnt;
-    const int c = cell_cost_class(box, g - box.base, cnt);
+    const int c = cell_items(box, g - box.base, npass);
     cls[g] = c;
-    if (c >= 0) atomicAdd(&sh[c], 1);
+    if (c >= 0) atomicAdd(&sh[c & 63], c >> 6);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kCostClasses; i += blockDim.x)
     if (sh[i]) atomicAdd(hist + i, sh[i]);
 }
 
-// hist[0..63] -> start offsets, heaviest class first; nitems = total
-// non-empty items.  One warp.
+// hist[0..63] -> start offsets, heaviest class first; nitems = total items.
+// One warp.
 __global__ void k_item_offsets(int* __restrict__ hist, int* __restrict__ start, int* __restrict__ nitems) {
   const int lane = threadIdx.x;
   // lane l owns classes 63 - 2l and 62 - 2l (descending order)
@@ -776,13 +813,20 @@ __global__ void k_item_offsets(int* __restrict__ hist, int* __restrict__ start, 
 }
 
 __global__ void k_item_scatter(const BoxCells* __restrict__ bc, int nbox, int total, const int* __restrict__ cls,
-                               const int* __restrict__ start, int* __restrict__ fill, int2* __restrict__ items) {
+                               const int* __restrict__ start, int* __restrict__ fill, int4* __restrict__ items) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= total) return;
   const int c = cls[g];
   if (c < 0) return;
   const int b = find_box(bc, nbox, g);
-  items[start[c] + atomicAdd(fill + c, 1)] = make_int2(b, g - __ldg(&bc[b].base));
+  const int key = g - __ldg(&bc[b].base);
+  const int k = c >> 6, cl = c & 63;
+  const int at = start[cl] + atomicAdd(fill + cl, k);
+  if (k == 1) {
+    items[at] = make_int4(b, key, 0, 0x7fffffff);
+  } else {
+    for (int p = 0; p < k; p++) items[at + p] = make_int4(b, key, p, p + 1);
+  }
 }
 
 }  // namespace
@@ -859,6 +903,9 @@ bool kick_shape_valid(const KickShape& k) {
          k.stage % 128 == 0 && pow2 && k.npass <= kPass && kick_smem(k) <= 200 * 1024;
 }
 
+int kick_queue_single(tpm_ctx* c, const KickArgs& a, const KickShape& k, int min_rung, double scale, double t0,
+                      int first_call, const int b[3], const int e[3]);
+
 int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0, int first_call) {
   if (!c->sorted) return fail(TPM_ERR_STATE, "kick_pme needs chainmesh_create first");
   if (!c->have_phi) return fail(TPM_ERR_STATE, "kick_pme needs gravity_long_compute first");
@@ -897,10 +944,13 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
   }
   stage_end(c, kStInterp);
   stage_begin(c, kStKick);
-  if (ncell > 0) {
+  if (ncell > 0 && c->opt.kick_grid) {
     kern<<<(unsigned)ncell, 32 * k.warps, smem, c->stream>>>(a, k.stage, k.npass);
     c->launches++;
     TPM_CUDA_TRY(cudaGetLastError());
+  } else if (ncell > 0) {
+    const int rc = kick_queue_single(c, a, k, min_rung, scale, t0, first_call, b, e);
+    if (rc) return rc;
   }
   stage_end(c, kStKick);
   c->pot_valid = min_rung <= 0 && ncell == (int64_t)C * C * C;
@@ -912,10 +962,11 @@ int kick_pme(tpm_ctx* c, const int box[6], int min_rung, double scale, double t0
 size_t kick_batch_args_bytes() { return sizeof(KickArgs); }
 size_t kick_batch_cells_bytes() { return sizeof(BoxCells); }
 
-int kick_batch_write_tables(tpm_ctx* const* boxes, int nbox, void* h_args, void* h_cells, int64_t* total_cells) {
+int kick_batch_write_tables(tpm_ctx* const* boxes, int nbox, void* h_args, void* h_cells, int64_t* total_cells,
+                            int64_t* max_items) {
   KickArgs* A = static_cast<KickArgs*>(h_args);
   BoxCells* B = static_cast<BoxCells*>(h_cells);
-  int64_t base = 0;
+  int64_t base = 0, parts = 0;
   for (int i = 0; i < nbox; i++) {
     tpm_ctx* c = boxes[i];
     const int b[3] = {0, 0, 0};
@@ -924,19 +975,28 @@ int kick_batch_write_tables(tpm_ctx* const* boxes, int nbox, void* h_args, void*
     B[i].begin = c->cell_begin;
     B[i].C = c->C;
     B[i].base = (int)base;
+    for (int d = 0; d < 3; d++) {
+      B[i].b[d] = 0;
+      B[i].e[d] = c->C;
+    }
     base += (int64_t)c->C * c->C * c->C;
+    parts += c->cap;
     if (base > 0x7fffffffLL) return fail(TPM_ERR_INVALID, "batch has more than 2^31 chain cells");
   }
   *total_cells = base;
+  // a cell of n sinks gives one item, or ceil(n / npass) >= 2 items when
+  // n > npass >= 8: at most one item per cell plus one per 8 particles
+  *max_items = base + parts / 8 + nbox;
+  if (*max_items > 0x7fffffffLL) return fail(TPM_ERR_INVALID, "batch has more than 2^31 work items");
   return TPM_OK;
 }
 
-int kick_batch_queue(const BatchQueue& q, cudaStream_t s) {
+int kick_batch_queue(const BatchQueue& q, int npass, cudaStream_t s) {
   if (q.total_cells <= 0) return TPM_OK;
   const int total = (int)q.total_cells;
   TPM_CUDA_TRY(cudaMemsetAsync(q.d_hist, 0, sizeof(int) * 2 * kCostClasses, s));
   const unsigned blocks = (unsigned)ceil_div(total, 256);
-  k_item_classes<<<blocks, 256, 0, s>>>(static_cast<const BoxCells*>(q.d_cells), q.nbox, total, q.d_class,
+  k_item_classes<<<blocks, 256, 0, s>>>(static_cast<const BoxCells*>(q.d_cells), q.nbox, total, npass, q.d_class,
                                         q.d_hist);
   k_item_offsets<<<1, 32, 0, s>>>(q.d_hist, q.d_hist + kCostClasses, q.d_nitems);
   k_item_scatter<<<blocks, 256, 0, s>>>(static_cast<const BoxCells*>(q.d_cells), q.nbox, total, q.d_class,
@@ -945,10 +1005,10 @@ int kick_batch_queue(const BatchQueue& q, cudaStream_t s) {
   return TPM_OK;
 }
 
-int kick_batch_interp(const BatchQueue& q, int min_rung, cudaStream_t s) {
+int kick_batch_interp(const BatchQueue& q, int min_rung, int npass, cudaStream_t s) {
   if (q.total_cells <= 0) return TPM_OK;
-  k_interp_batch<<<(unsigned)q.total_cells, 64, 0, s>>>(static_cast<const KickArgs*>(q.d_args), q.d_items,
-                                                         q.d_nitems, min_rung);
+  k_interp_batch<<<(unsigned)q.max_items, 64, 0, s>>>(static_cast<const KickArgs*>(q.d_args), q.d_items,
+                                                       q.d_nitems, min_rung, npass);
   TPM_CUDA_TRY(cudaGetLastError());
   return TPM_OK;
 }
@@ -965,7 +1025,7 @@ int kick_batch_kick(const BatchQueue& q, const KickShape& k, bool wrap, int min_
   TPM_CUDA_TRY(cudaGetDevice(&dev));
   TPM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   if (per_sm < 1) return fail(TPM_ERR_INVALID, "kick shape does not fit on an SM");
-  const int64_t blocks = std::min<int64_t>((int64_t)per_sm * sms, q.total_cells);
+  const int64_t blocks = std::min<int64_t>((int64_t)per_sm * sms, q.max_items);
   StepScalars st{min_rung, first_call ? 1 : 0, (float)t0, (float)scale};
   TPM_CUDA_TRY(cudaMemsetAsync(q.d_counter, 0, sizeof(int), s));
   kern<<<(unsigned)blocks, 32 * k.warps, smem, s>>>(static_cast<const KickArgs*>(q.d_args), q.d_items, q.d_nitems,
@@ -973,6 +1033,51 @@ int kick_batch_kick(const BatchQueue& q, const KickShape& k, bool wrap, int min_
   TPM_CUDA_TRY(cudaGetLastError());
   if (blocks_out) *blocks_out = (int)blocks;
   return TPM_OK;
+}
+
+// The single-box kick through the same persistent queue: heavy cells split
+// into pass items, so a strongly clustered box is spread over every SM.
+int kick_queue_single(tpm_ctx* c, const KickArgs& a, const KickShape& k, int min_rung, double scale, double t0,
+                      int first_call, const int b[3], const int e[3]) {
+  BatchQueue& q = c->kq;
+  const int64_t ncell = (int64_t)c->C * c->C * c->C;
+  if (!q.d_args) {
+    q.nbox = 1;
+    q.total_cells = ncell;
+    q.max_items = ncell + c->cap / 8 + 1;
+    if (q.max_items > 0x7fffffffLL) return fail(TPM_ERR_INVALID, "more than 2^31 work items");
+    cudaError_t err = cudaMalloc(&q.d_args, sizeof(KickArgs));
+    if (err == cudaSuccess) err = cudaMalloc(&q.d_cells, sizeof(BoxCells));
+    if (err == cudaSuccess) err = cudaMalloc((void**)&q.d_class, sizeof(int) * ncell);
+    if (err == cudaSuccess) err = cudaMalloc((void**)&q.d_hist, sizeof(int) * 2 * kCostClasses);
+    if (err == cudaSuccess) err = cudaMalloc((void**)&q.d_items, sizeof(int4) * q.max_items);
+    if (err == cudaSuccess) err = cudaMalloc((void**)&q.d_nitems, sizeof(int) * 2);
+    if (err == cudaSuccess) err = cudaMalloc((void**)&q.d_counter, sizeof(int) * 2);
+    if (err != cudaSuccess) {
+      cudaGetLastError();
+      return fail(TPM_ERR_NOMEM, std::string("kick queue: ") + cudaGetErrorString(err));
+    }
+    c->device_bytes += sizeof(KickArgs) + sizeof(BoxCells) + 4 * ncell + 8 * kCostClasses + 16 * q.max_items + 16;
+  }
+  // per-call arguments: array addresses move with the sort's buffer swaps
+  KickArgs* ha = reinterpret_cast<KickArgs*>(c->kq_host_args);
+  BoxCells* hb = reinterpret_cast<BoxCells*>(c->kq_host_cells);
+  static_assert(sizeof(KickArgs) <= sizeof(c->kq_host_args), "host argument buffer too small");
+  static_assert(sizeof(BoxCells) <= sizeof(c->kq_host_cells), "host cell-table buffer too small");
+  *ha = a;
+  hb->begin = c->cell_begin;
+  hb->C = c->C;
+  hb->base = 0;
+  for (int d = 0; d < 3; d++) {
+    hb->b[d] = b[d];
+    hb->e[d] = e[d];
+  }
+  TPM_CUDA_TRY(cudaMemcpyAsync(q.d_args, ha, sizeof(KickArgs), cudaMemcpyHostToDevice, c->stream));
+  TPM_CUDA_TRY(cudaMemcpyAsync(q.d_cells, hb, sizeof(BoxCells), cudaMemcpyHostToDevice, c->stream));
+  int rc = kick_batch_queue(q, k.npass, c->stream);
+  if (rc == TPM_OK) rc = kick_batch_kick(q, k, c->C == 3, min_rung, scale, t0, first_call, c->stream, nullptr);
+  c->launches += 4;
+  return rc;
 }
 
 }  // namespace tpm

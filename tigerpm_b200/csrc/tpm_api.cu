@@ -401,6 +401,10 @@ int tpm_ctx_destroy(tpm_ctx* c) {
                   c->thr, c->tree, c->depth1d, c->fft_tw, c->gtab, c->k2tab, c->d_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  void* kq[] = {c->kq.d_args, c->kq.d_cells, c->kq.d_class, c->kq.d_hist, c->kq.d_items, c->kq.d_nitems,
+                c->kq.d_counter};
+  for (void* p : kq)
+    if (p) cudaFree(p);
   // a borrowed working set (served boxes) belongs to its lender
   if (c->has_scratch)
     for (const auto& f : scratch_fields(c))
@@ -453,10 +457,12 @@ static int set_common(tpm_ctx* c, int64_t n, cudaMemcpyKind kind, const uint32_t
     else TPM_CUDA_TRY(cudaMemsetAsync(c->vz, 0, 4 * n, s));
     if (rung) TPM_CUDA_TRY(cudaMemcpyAsync(c->rung, rung, n, kind, s));
     else TPM_CUDA_TRY(cudaMemsetAsync(c->rung, 0, n, s));
-    TPM_CUDA_TRY(cudaMemsetAsync(c->gx, 0, 4 * n, s));
-    TPM_CUDA_TRY(cudaMemsetAsync(c->gy, 0, 4 * n, s));
-    TPM_CUDA_TRY(cudaMemsetAsync(c->gz, 0, 4 * n, s));
-    TPM_CUDA_TRY(cudaMemsetAsync(c->pot, 0, 4 * n, s));
+    if (c->gx) {  // a served box has no force arrays between steps
+      TPM_CUDA_TRY(cudaMemsetAsync(c->gx, 0, 4 * n, s));
+      TPM_CUDA_TRY(cudaMemsetAsync(c->gy, 0, 4 * n, s));
+      TPM_CUDA_TRY(cudaMemsetAsync(c->gz, 0, 4 * n, s));
+      TPM_CUDA_TRY(cudaMemsetAsync(c->pot, 0, 4 * n, s));
+    }
   }
   c->sorted = false;
   c->have_phi = false;

@@ -59,6 +59,20 @@ struct StageEvents {
   int64_t count[kNumStages];  // records since the last reset
 };
 
+// Work queue of a persistent kick over one or many boxes (device arrays).
+struct BatchQueue {
+  int nbox = 0;
+  int64_t total_cells = 0;   // sum of the boxes' chain cells
+  int64_t max_items = 0;     // capacity of d_items
+  void* d_args = nullptr;    // per-box kernel arguments (kick_batch_args_bytes each)
+  void* d_cells = nullptr;   // per-box cell tables (kick_batch_cells_bytes each)
+  int* d_class = nullptr;    // cost class | items << 6 of every (box, cell), total_cells
+  int* d_hist = nullptr;     // 2 x 64 ints
+  int4* d_items = nullptr;   // (box, cell key, first pass, end pass), heaviest first
+  int* d_nitems = nullptr;   // items in use
+  int* d_counter = nullptr;  // persistent-kernel work counter
+};
+
 }  // namespace tpm
 
 struct tpm_ctx {
@@ -136,6 +150,11 @@ struct tpm_ctx {
   // pot holds every particle's potential in the current order (a kick of
   // the whole box with min_rung 0 since the last sort)
   bool pot_valid = false;
+  // the single-box kick's work queue (allocated on the first kick) and the
+  // host copies of its one-box argument and cell tables
+  tpm::BatchQueue kq;
+  alignas(16) unsigned char kq_host_args[256];
+  alignas(16) unsigned char kq_host_cells[64];
   // big-step integrator state (integrate.cu): ticks of t0 / 2^31
   double int_t0 = 0, int_scale = 1;
   int64_t int_tick = 0;
@@ -163,22 +182,12 @@ KickShape kick_default_shape(double mean_cell);
 bool kick_shape_valid(const KickShape& k);
 
 // Work queue of a batched kick over many boxes (device arrays).
-struct BatchQueue {
-  int nbox = 0;
-  int64_t total_cells = 0;   // sum of the boxes' chain cells
-  void* d_args = nullptr;    // per-box kernel arguments (kick_batch_args_bytes each)
-  void* d_cells = nullptr;   // per-box cell tables (kick_batch_cells_bytes each)
-  int* d_class = nullptr;    // cost class of every (box, cell), total_cells
-  int* d_hist = nullptr;     // 2 x 64 ints
-  int2* d_items = nullptr;   // (box, cell key), heaviest first, total_cells
-  int* d_nitems = nullptr;   // non-empty items
-  int* d_counter = nullptr;  // persistent-kernel work counter
-};
 size_t kick_batch_args_bytes();
 size_t kick_batch_cells_bytes();
-int kick_batch_write_tables(tpm_ctx* const* boxes, int nbox, void* h_args, void* h_cells, int64_t* total_cells);
-int kick_batch_queue(const BatchQueue& q, cudaStream_t s);
-int kick_batch_interp(const BatchQueue& q, int min_rung, cudaStream_t s);
+int kick_batch_write_tables(tpm_ctx* const* boxes, int nbox, void* h_args, void* h_cells, int64_t* total_cells,
+                            int64_t* max_items);
+int kick_batch_queue(const BatchQueue& q, int npass, cudaStream_t s);
+int kick_batch_interp(const BatchQueue& q, int min_rung, int npass, cudaStream_t s);
 int kick_batch_kick(const BatchQueue& q, const KickShape& k, bool wrap, int min_rung, double scale, double t0,
                     int first_call, cudaStream_t s, int* blocks_out);
 
