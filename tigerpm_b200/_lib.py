@@ -44,7 +44,7 @@ class Options(C.Structure):
         ("z0", C.c_double),
         ("rcut_over_rs", C.c_double), ("assign", C.c_int), ("deconv_order", C.c_int),
         ("sort_mode", C.c_int), ("kahan", C.c_int), ("deterministic_deposit", C.c_int),
-        ("fft", C.c_int), ("seed", C.c_uint64), ("kick_grid", C.c_int),
+        ("fft", C.c_int), ("seed", C.c_uint64), ("fft_group", C.c_int), ("kick_grid", C.c_int),
     ]
 
 

@@ -228,15 +228,16 @@ __device__ __forceinline__ void load_twiddles(float2* s_tw, const float2* __rest
 // P1: forward z transform of real rows (x, 2p) and (x, 2p+1) as one complex
 // line, then A_k = (Z_k + conj Z_{N-k}) / 2, B_k = (Z_k - conj Z_{N-k}) / 2i.
 __global__ void __launch_bounds__(kFftThreads) k_fft_z_r2c(const float* __restrict__ rho, float2* __restrict__ Y,
-                                                           FftPlan p, const float2* __restrict__ tw) {
+                                                           FftPlan p, const float2* __restrict__ tw, int x0) {
   extern __shared__ float2 fsm[];
   const int N = p.N, LS = line_stride(N), Nh = N / 2 + 1;
   float2* buf = fsm;
   float2* alt = fsm + kFftLines * LS;
   float2* s_tw = fsm + 2 * kFftLines * LS;
   const int per_x = N / (2 * kFftLines);
-  const int x = blockIdx.x / per_x;
-  const int p0 = (blockIdx.x - x * per_x) * kFftLines;
+  const int xb = blockIdx.x / per_x;
+  const int x = x0 + xb;
+  const int p0 = (blockIdx.x - xb * per_x) * kFftLines;
 #pragma unroll 1
   for (int l = 0; l < kFftLines; l++) {
     const int64_t row = (int64_t)x * N + 2 * (p0 + l);
@@ -267,15 +268,16 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_z_r2c(const float* __restri
 // P2 / P4: transform along y of the L kz columns [c0, c0 + L) of plane x.
 template <int S>
 __global__ void __launch_bounds__(kFftThreads) k_fft_y(float2* __restrict__ Y, FftPlan p,
-                                                       const float2* __restrict__ tw) {
+                                                       const float2* __restrict__ tw, int x0) {
   extern __shared__ float2 fsm[];
   const int N = p.N, LS = line_stride(N);
   float2* buf = fsm;
   float2* alt = fsm + kFftLines * LS;
   float2* s_tw = fsm + 2 * kFftLines * LS;
   const int per_x = p.Sz / kFftLines;
-  const int x = blockIdx.x / per_x;
-  const int c0 = (blockIdx.x - x * per_x) * kFftLines;
+  const int xb = blockIdx.x / per_x;
+  const int x = x0 + xb;
+  const int c0 = (blockIdx.x - xb * per_x) * kFftLines;
   float2* plane = Y + (int64_t)x * N * p.Sz + c0;
   for (int e = threadIdx.x; e < kFftLines * N; e += kFftThreads) {
     const int y = e / kFftLines, c = e - y * kFftLines;
@@ -341,15 +343,16 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_x_green(float2* __restrict_
 // A_{N-k} = conj A_k (imaginary parts of k = 0 and N/2 dropped, as a real
 // transform has none), inverse FFT, real part -> row 2p, imaginary -> 2p+1.
 __global__ void __launch_bounds__(kFftThreads) k_fft_z_c2r(const float2* __restrict__ Y, float* __restrict__ phi,
-                                                           FftPlan p, const float2* __restrict__ tw) {
+                                                           FftPlan p, const float2* __restrict__ tw, int x0) {
   extern __shared__ float2 fsm[];
   const int N = p.N, LS = line_stride(N), Nh2 = N / 2;
   float2* buf = fsm;
   float2* alt = fsm + kFftLines * LS;
   float2* s_tw = fsm + 2 * kFftLines * LS;
   const int per_x = N / (2 * kFftLines);
-  const int x = blockIdx.x / per_x;
-  const int p0 = (blockIdx.x - x * per_x) * kFftLines;
+  const int xb = blockIdx.x / per_x;
+  const int x = x0 + xb;
+  const int p0 = (blockIdx.x - xb * per_x) * kFftLines;
 #pragma unroll 1
   for (int l = 0; l < kFftLines; l++) {
     const int64_t row = (int64_t)x * N + 2 * (p0 + l);
@@ -407,6 +410,28 @@ bool plan_radices(int N, FftPlan& p) {
 
 size_t fft_smem(int N) { return sizeof(float2) * (2 * (size_t)kFftLines * (N + 16 / kFftLines) + N); }
 
+// The dynamic shared-memory limit of the transform kernels is one setting
+// per kernel for the whole process, so it is set before every solve: a
+// context with a smaller mesh must not lower it for another one.
+int set_fft_smem(size_t smem) {
+  TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_green, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return TPM_OK;
+}
+
+// x-planes per launch of the z / y passes: the fft_group option, else as
+// many planes as keep their spectrum (N * Sz complex each) within a quarter
+// of L2 (a whole pass when the spectrum fits).
+int plane_group(const tpm_ctx* c, int N) {
+  if (c->opt.fft_group > 0) return std::min(c->opt.fft_group, N);
+  const double plane = 8.0 * N * (double)fft3d_padded_columns(N);
+  const int g = (int)std::max(1.0, std::floor(32.0 * 1024 * 1024 / plane));
+  return std::min(g, N);
+}
+
 }  // namespace
 
 int fft3d_padded_columns(int N) { return ((N / 2 + 1) + kFftLines - 1) / kFftLines * kFftLines; }
@@ -427,12 +452,7 @@ int fft3d_init(tpm_ctx* c) {
   // padding columns stay zero: the transforms keep them zero and never store them into phi
   if (c->rhok) TPM_CUDA_TRY(cudaMemset(c->rhok, 0, sizeof(float2) * (size_t)N * N * fft3d_padded_columns(N)));
   const int smem = (int)fft_smem(N);
-  TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_green, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  TPM_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  return TPM_OK;
+  return set_fft_smem(smem);
 }
 
 int fft3d_poisson(tpm_ctx* c, const float* gt) {
@@ -442,22 +462,39 @@ int fft3d_poisson(tpm_ctx* c, const float* gt) {
   p.Sz = fft3d_padded_columns(N);
   float2* Y = reinterpret_cast<float2*>(c->rhok);
   const size_t smem = fft_smem(N);
+  const int rca = set_fft_smem(smem);
+  if (rca) return rca;
   cudaStream_t s = c->stream;
   const unsigned zblocks = (unsigned)(N * (N / (2 * kFftLines)));
   const unsigned cblocks = (unsigned)(N * (p.Sz / kFftLines));
   const float norm = (float)(1.0 / ((double)N * N * N));
   stage_begin(c, kStFftF);
-  k_fft_z_r2c<<<zblocks, kFftThreads, smem, s>>>(c->rho, Y, p, c->fft_tw);
-  k_fft_y<-1><<<cblocks, kFftThreads, smem, s>>>(Y, p, c->fft_tw);
+  // The z and y passes work plane by plane in x: launched a group of planes
+  // at a time, the spectrum one z pass writes is still in L2 when the y pass
+  // reads it (and the inverse y pass output when the z pass reads it), so
+  // those intermediates make no round trip through HBM.
+  const int G = plane_group(c, N);
+  const unsigned zper = (unsigned)(N / (2 * kFftLines)), cper = (unsigned)(p.Sz / kFftLines);
+  for (int x0 = 0; x0 < N; x0 += G) {
+    const int g = std::min(G, N - x0);
+    k_fft_z_r2c<<<zper * g, kFftThreads, smem, s>>>(c->rho, Y, p, c->fft_tw, x0);
+    k_fft_y<-1><<<cper * g, kFftThreads, smem, s>>>(Y, p, c->fft_tw, x0);
+    c->launches += 2;
+  }
+  (void)zblocks;
   stage_end(c, kStFftF);
   stage_begin(c, kStGreen);
   k_fft_x_green<<<cblocks, kFftThreads, smem, s>>>(Y, p, c->fft_tw, gt, c->k2tab, norm);
   stage_end(c, kStGreen);
   stage_begin(c, kStFftI);
-  k_fft_y<1><<<cblocks, kFftThreads, smem, s>>>(Y, p, c->fft_tw);
-  k_fft_z_c2r<<<zblocks, kFftThreads, smem, s>>>(Y, c->phi, p, c->fft_tw);
+  for (int x0 = 0; x0 < N; x0 += G) {
+    const int g = std::min(G, N - x0);
+    k_fft_y<1><<<cper * g, kFftThreads, smem, s>>>(Y, p, c->fft_tw, x0);
+    k_fft_z_c2r<<<zper * g, kFftThreads, smem, s>>>(Y, c->phi, p, c->fft_tw, x0);
+    c->launches += 2;
+  }
   stage_end(c, kStFftI);
-  c->launches += 5;
+  c->launches += 1;
   TPM_CUDA_TRY(cudaGetLastError());
   return TPM_OK;
 }

@@ -131,6 +131,57 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
   // cancelling it away (the weights sum to one, so phi adds it back).
   const float pc = __ldg(a.phi + (int64_t)wrapi(base[0] + 2, N) * N * N + iy[2] + iz[2]);
   float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+  const int z0 = iz[0];
+  const int a4 = z0 & ~3;
+  if ((N & 3) == 0 && a4 + 12 <= N) {
+    // Each z-run of 6 points is read as three aligned float4 (12 points
+    // from a4 = z0 rounded down to 4); the z weights are shifted by
+    // s = z0 - a4 once per sink, zero outside the run.
+    const int s = z0 - a4;
+    float ws[12], dws[12];
+#pragma unroll
+    for (int m = 0; m < 12; m++) {
+      float u = 0.f, du = 0.f;
+#pragma unroll
+      for (int k = 0; k < kNInterp; k++) {
+        const bool hit = m - k == s;
+        u = hit ? w[2][k] : u;
+        du = hit ? dw[2][k] : du;
+      }
+      ws[m] = u;
+      dws[m] = du;
+    }
+#pragma unroll 1
+    for (int i = 0; i < kNInterp; i++) {
+      const int64_t plane = (int64_t)wrapi(base[0] + i, N) * N * N;
+      float px = 0.f, py = 0.f, pz = 0.f;
+#pragma unroll
+      for (int j = 0; j < kNInterp; j++) {
+        const float4* row = reinterpret_cast<const float4*>(a.phi + plane + iy[j] + a4);
+        const float4 f0 = __ldg(row), f1 = __ldg(row + 1), f2 = __ldg(row + 2);
+        const float v[12] = {f0.x - pc, f0.y - pc, f0.z - pc, f0.w - pc, f1.x - pc, f1.y - pc,
+                             f1.z - pc, f1.w - pc, f2.x - pc, f2.y - pc, f2.z - pc, f2.w - pc};
+        float rz = 0.f, rdz = 0.f;
+#pragma unroll
+        for (int m = 0; m < 12; m++) {
+          rz = fmaf(ws[m], v[m], rz);
+          rdz = fmaf(dws[m], v[m], rdz);
+        }
+        px = fmaf(w[1][j], rz, px);
+        py = fmaf(dw[1][j], rz, py);
+        pz = fmaf(w[1][j], rdz, pz);
+      }
+      sx = fmaf(dw[0][i], px, sx);
+      sy = fmaf(w[0][i], py, sy);
+      sz = fmaf(w[0][i], pz, sz);
+      sp = fmaf(w[0][i], px, sp);
+    }
+    lx = -sx * (float)N;
+    ly = -sy * (float)N;
+    lz = -sz * (float)N;
+    lp = sp + pc;
+    return;
+  }
   for (int i = 0; i < kNInterp; i++) {
     const int64_t plane = (int64_t)wrapi(base[0] + i, N) * N * N;
     float px = 0.f, py = 0.f, pz = 0.f;

@@ -63,6 +63,7 @@ struct ServeReq {
   double dt = 0, scale = 1, t0 = 1;
   int min_rung = 0, first_call = 1;
   int status = TPM_OK;
+  std::string msg;  // the failing call's message (set on the dispatcher thread)
   double t_submit = 0, t_start = 0, t_done = 0;
   float device_ms = 0;
   bool done = false;
@@ -130,6 +131,7 @@ int issue(tpm_server* s, int k, const ServeReq& rq, std::vector<CallbackArg>& cb
   ServeBox& bx = s->boxes[rq.box];
   tpm_ctx* c = bx.c;
   int rc = TPM_OK;
+  cudaGetLastError();  // a step reports only its own errors
   cudaError_t e = cudaMallocFromPoolAsync(&sl.mem, (size_t)bx.scratch, s->pool, sl.s);
   if (e != cudaSuccess) {
     sl.mem = nullptr;
@@ -233,6 +235,7 @@ void dispatcher(tpm_server* s) {
         if (rc != TPM_OK) {
           std::lock_guard<std::mutex> g(s->mu);
           s->reqs[start_ids[j]].status = rc;
+          s->reqs[start_ids[j]].msg = tpm_last_error_message();
         }
       }
       lock.lock();
@@ -432,7 +435,8 @@ int tpm_serve_wait(tpm_server* s, int req, tpm_serve_result* out) {
     out->device_ms = r.device_ms;
     out->particles = s->boxes[r.box].c->n;
   }
-  return r.status == TPM_OK ? TPM_OK : fail(r.status, "served step " + std::to_string(req) + " failed");
+  return r.status == TPM_OK ? TPM_OK
+                            : fail(r.status, "served step " + std::to_string(req) + " failed: " + r.msg);
 }
 
 int tpm_serve_drain(tpm_server* s) {
