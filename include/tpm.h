@@ -104,7 +104,8 @@ typedef struct tpm_options {
   int fft;             /* TPM_FFT_*: 3-D transforms of gravity_long_compute */
   uint64_t seed;       /* synthetic-input seed carried for drivers */
   int fft_group;       /* x-planes per launch of the library FFT's z / y passes
-                        * (0: as many as keep their spectrum in a quarter of L2) */
+                        * (0: all; smaller groups keep the spectrum in L2 between
+                        * the two passes) */
   int kick_grid;       /* 0: the PP + kick as one persistent launch over a cost-sorted
                         * queue of (cell, sink pass) items (default; balances clustered
                         * boxes); 1: one block per sink cell */

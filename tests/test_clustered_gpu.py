@@ -51,7 +51,9 @@ def run(opts, ps, kick_grid):
 def test_heavy_cell_queue_matches_grid_and_oracle():
     n = 48
     p = W.accurate_box_params(n)
-    opts = make_options(n, p["grid"], rs_cells=p["rs_cells"], rcut_over_rs=p["rcut_over_rs"], assign="cloud4")
+    # the exact deposit: both launch forms must see the same potential bits
+    opts = make_options(n, p["grid"], rs_cells=p["rs_cells"], rcut_over_rs=p["rcut_over_rs"], assign="cloud4",
+                        deterministic_deposit=True)
     ps = clumped(n, 40000, 5)
     before, phi, after_q, forces_q, offs = run(opts, ps, 0)
     counts = np.diff(offs)

@@ -422,14 +422,13 @@ int set_fft_smem(size_t smem) {
   return TPM_OK;
 }
 
-// x-planes per launch of the z / y passes: the fft_group option, else as
-// many planes as keep their spectrum (N * Sz complex each) within a quarter
-// of L2 (a whole pass when the spectrum fits).
+// x-planes per launch of the z / y passes: the fft_group option, else all
+// of them.  Groups whose spectrum stays in L2 between the two passes were
+// measured slower at 768^3 (13 planes: z + y forward 4.22 ms against 3.21 ms
+// as whole passes): the short launches leave partial waves and gaps.
 int plane_group(const tpm_ctx* c, int N) {
   if (c->opt.fft_group > 0) return std::min(c->opt.fft_group, N);
-  const double plane = 8.0 * N * (double)fft3d_padded_columns(N);
-  const int g = (int)std::max(1.0, std::floor(32.0 * 1024 * 1024 / plane));
-  return std::min(g, N);
+  return N;
 }
 
 }  // namespace

@@ -111,65 +111,12 @@ struct DepAcc<false> {
   static __device__ __forceinline__ double value(T v, double scale) { return (double)v * scale; }
 };
 
-// Per-warp queue of particles to deposit: 64 entries of int4 after the tile.
-constexpr int kDepQueue = 64;
-template <int T, bool EXACT>
-__host__ __device__ constexpr size_t dep_queue_offset() {
-  return (sizeof(typename DepAcc<EXACT>::T) * T * T * T + 15) / 16 * 16;
-}
-template <int T, bool EXACT>
-constexpr size_t dep_smem_bytes() {
-  return dep_queue_offset<T, EXACT>() + sizeof(int4) * kDepQueue * (256 / 32);
-}
-
-// Adds one particle's assignment weights to the tile points it reaches.
-template <int T, int ASSIGN, bool EXACT>
-__device__ __forceinline__ void deposit_one(int4 q, const int o[3], const int ext[3], int N,
-                                            typename DepAcc<EXACT>::T* acc) {
-  constexpr int W = Width<ASSIGN>::W;
-  using A = DepAcc<EXACT>;
-  float wx[4], wy[4], wz[4];
-  int r[3];
-  r[0] = stencil<ASSIGN>((uint32_t)q.x, N, wx) - o[0];
-  r[1] = stencil<ASSIGN>((uint32_t)q.y, N, wy) - o[1];
-  r[2] = stencil<ASSIGN>((uint32_t)q.z, N, wz) - o[2];
-  int li[3][4];
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-#pragma unroll
-    for (int k = 0; k < W; k++) {
-      int l = r[d] + k;
-      if (l < 0) l += N;
-      else if (l >= N) l -= N;
-      li[d][k] = l < ext[d] ? l : -1;
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < W; i++) {
-    if (li[0][i] < 0) continue;
-#pragma unroll
-    for (int j = 0; j < W; j++) {
-      if (li[1][j] < 0) continue;
-      const float wxy = wx[i] * wy[j];
-      typename A::T* row_acc = acc + (li[0][i] * T + li[1][j]) * T;
-#pragma unroll
-      for (int k = 0; k < W; k++) {
-        if (li[2][k] < 0) continue;
-        A::add(row_acc + li[2][k], wxy * wz[k]);
-      }
-    }
-  }
-}
-
 template <int T, int ASSIGN, bool EXACT>
 __global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
   constexpr int W = Width<ASSIGN>::W;
   using A = DepAcc<EXACT>;
   extern __shared__ __align__(16) unsigned char dep_smem[];
   typename A::T* acc = reinterpret_cast<typename A::T*>(dep_smem);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int4* wq = reinterpret_cast<int4*>(dep_smem + dep_queue_offset<T, EXACT>()) + warp * kDepQueue;
-  int qn = 0;
   const int N = a.N, C = a.C;
   int tb = blockIdx.x;
   const int tz = tb % a.ntile;
@@ -209,40 +156,56 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
           cb = xend - C;
         }
         const int32_t pb = __ldg(a.begin + row + ca), pe = __ldg(a.begin + row + cb);
-        // warp-uniform sweep: the particles whose stencils reach the tile are
-        // compacted into the warp's queue, and each full queue is deposited
-        // with every lane busy (most particles of the outer cells miss it)
-        for (int32_t base = pb + warp * 32; base < pe; base += blockDim.x) {
-          const int32_t p = base + lane;
-          bool t = false;
-          int4 q = make_int4(0, 0, 0, 0);
-          if (p < pe) {
-            q = __ldg(a.pos4 + p);
-            // first stencil point per dim relative to the tile, wrapped into
-            // [-N/2, N/2): the particle touches the tile only if every dim's
-            // W points meet [0, ext)
-            const int s0 = (int)(((uint64_t)(uint32_t)q.x * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
-            const int s1 = (int)(((uint64_t)(uint32_t)q.y * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
-            const int s2 = (int)(((uint64_t)(uint32_t)q.z * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
-            t = touches<W>(s0 - o[0], N, ext[0]) && touches<W>(s1 - o[1], N, ext[1]) &&
-                touches<W>(s2 - o[2], N, ext[2]);
+        for (int32_t p = pb + threadIdx.x; p < pe; p += blockDim.x) {
+          const int4 q = __ldg(a.pos4 + p);
+          // first stencil point per dim relative to the tile, wrapped into
+          // [-N/2, N/2): the particle touches the tile only if every dim's
+          // W points meet [0, ext)
+          const int s0 = (int)(((uint64_t)(uint32_t)q.x * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
+          const int s1 = (int)(((uint64_t)(uint32_t)q.y * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
+          const int s2 = (int)(((uint64_t)(uint32_t)q.z * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
+          if (!touches<W>(s0 - o[0], N, ext[0]) || !touches<W>(s1 - o[1], N, ext[1]) ||
+              !touches<W>(s2 - o[2], N, ext[2]))
+            continue;
+          float wx[4], wy[4], wz[4];
+          int r[3];
+          r[0] = stencil<ASSIGN>((uint32_t)q.x, N, wx) - o[0];
+          r[1] = stencil<ASSIGN>((uint32_t)q.y, N, wy) - o[1];
+          r[2] = stencil<ASSIGN>((uint32_t)q.z, N, wz) - o[2];
+          int li[3][4];
+          bool any = true;
+          for (int d = 0; d < 3; d++) {
+            bool hit = false;
+#pragma unroll
+            for (int k = 0; k < W; k++) {
+              int l = r[d] + k;
+              if (l < 0) l += N;
+              else if (l >= N) l -= N;
+              li[d][k] = l < ext[d] ? l : -1;
+              hit |= l < ext[d];
+            }
+            any &= hit;
           }
-          const unsigned m = __ballot_sync(0xffffffffu, t);
-          if (t) wq[qn + __popc(m & ((1u << lane) - 1u))] = q;
-          qn += __popc(m);
-          __syncwarp();
-          if (qn >= 32) {
-            deposit_one<T, ASSIGN, EXACT>(wq[lane], o, ext, N, acc);
-            __syncwarp();
-            if (lane < qn - 32) wq[lane] = wq[32 + lane];
-            qn -= 32;
-            __syncwarp();
+          if (!any) continue;
+#pragma unroll
+          for (int i = 0; i < W; i++) {
+            if (li[0][i] < 0) continue;
+#pragma unroll
+            for (int j = 0; j < W; j++) {
+              if (li[1][j] < 0) continue;
+              const float wxy = wx[i] * wy[j];
+              typename A::T* row_acc = acc + (li[0][i] * T + li[1][j]) * T;
+#pragma unroll
+              for (int k = 0; k < W; k++) {
+                if (li[2][k] < 0) continue;
+                A::add(row_acc + li[2][k], wxy * wz[k]);
+              }
+            }
           }
         }
       }
     }
   }
-  if (lane < qn) deposit_one<T, ASSIGN, EXACT>(wq[lane], o, ext, N, acc);
   __syncthreads();
   for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) {
     const int lz = i % T, ly = (i / T) % T, lx = i / (T * T);
@@ -325,7 +288,7 @@ template <int T, bool EXACT>
 int launch_deposit_T(tpm_ctx* c, DepositArgs a) {
   a.ntile = ceil_div(c->N, T);
   const int blocks = a.ntile * a.ntile * a.ntile;
-  const size_t smem = dep_smem_bytes<T, EXACT>();
+  const size_t smem = sizeof(typename DepAcc<EXACT>::T) * T * T * T;
   a.scale = 4.0 * M_PI * c->N * (EXACT ? std::ldexp(1.0, -kDepositFracBits) : 1.0);
   switch (c->opt.assign) {
     case TPM_ASSIGN_CIC:

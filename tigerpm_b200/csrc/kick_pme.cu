@@ -720,10 +720,13 @@ __device__ __forceinline__ KickArgs box_args(const KickArgs* __restrict__ boxes,
   return a;
 }
 
-template <bool WRAP>
+// SINGLE: one box whose arguments come as the kernel parameter `one` (the
+// constant bank, like the per-cell launch); else per-box arguments from
+// `boxes`, kept in shared memory.
+template <bool WRAP, bool SINGLE>
 __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB)
-    k_kick_batch(const KickArgs* __restrict__ boxes, const int4* __restrict__ items, const int* __restrict__ nitems,
-                 int* __restrict__ counter, StepScalars st, int stage, int npass) {
+    k_kick_batch(const KickArgs* __restrict__ boxes, KickArgs one, const int4* __restrict__ items,
+                 const int* __restrict__ nitems, int* __restrict__ counter, StepScalars st, int stage, int npass) {
   extern __shared__ float4 smem4[];
   __shared__ int s_item[2];
   // The box's arguments are read from shared memory where they are used:
@@ -739,14 +742,21 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB)
     // the next item is fetched while this one runs; the barrier at the end of
     // the iteration orders the write against the reads of s_item[k ^ 1]
     if (threadIdx.x == 0) s_item[k ^ 1] = atomicAdd(counter, 1);
-    const int4 w = __ldg(items + it);  // (box, cell key, first pass, end pass)
-    if (w.x != cur_box) {  // uniform: every thread read the same item
-      if (threadIdx.x == 0) s_args = box_args(boxes, w.x, st);
-      cur_box = w.x;
-      __syncthreads();
+    const int4 w = __ldg(items + it);  // (box, cell key, first pass, end pass); box -1: empty slot
+    if (w.x >= 0) {  // uniform: every thread read the same item
+      if (SINGLE) {
+        const int C = one.C;
+        kick_cell<WRAP>(one, w.y % C, (w.y / C) % C, w.y / (C * C), smem4, stage, npass, w.z, w.w);
+      } else {
+        if (w.x != cur_box) {
+          if (threadIdx.x == 0) s_args = box_args(boxes, w.x, st);
+          cur_box = w.x;
+          __syncthreads();
+        }
+        const int C = s_args.C;
+        kick_cell<WRAP>(s_args, w.y % C, (w.y / C) % C, w.y / (C * C), smem4, stage, npass, w.z, w.w);
+      }
     }
-    const int C = s_args.C;
-    kick_cell<WRAP>(s_args, w.y % C, (w.y / C) % C, w.y / (C * C), smem4, stage, npass, w.z, w.w);
     __syncthreads();
   }
 }
@@ -757,6 +767,7 @@ __global__ void __launch_bounds__(64) k_interp_batch(const KickArgs* __restrict_
                                                       const int* __restrict__ nitems, int min_rung, int npass) {
   if ((int)blockIdx.x >= *nitems) return;
   const int4 w = __ldg(items + blockIdx.x);
+  if (w.x < 0) return;  // empty slot
   const KickArgs& a = boxes[w.x];
   const int32_t pb = __ldg(a.begin + w.y), pe = __ldg(a.begin + w.y + 1);
   int np = 8;
@@ -797,6 +808,8 @@ __device__ __forceinline__ int find_box(const BoxCells* __restrict__ bc, int nbo
 }
 
 constexpr int kCostClasses = 64;
+// A cell needing more sink passes than this becomes one item per pass.
+constexpr int kSplitPasses = 4;
 
 // Items of one cell: none outside the kick box or when empty; one item per
 // sink pass (np = the power of two >= the cell's count, at most npass) when
@@ -821,8 +834,9 @@ __device__ __forceinline__ int cell_items(const BoxCells& b, int key, int npass)
   int np = 8;
   while (np < npass && np < n) np <<= 1;
   const int passes = (n + np - 1) / np;
-  const uint64_t cost = (uint64_t)min(n, np) * (uint64_t)nb;
-  return (63 - __clzll((long long)(cost | 1ull))) | (passes << 6);
+  const int items = passes > kSplitPasses ? passes : 1;
+  const uint64_t cost = (uint64_t)(items > 1 ? np : n) * (uint64_t)nb;
+  return (63 - __clzll((long long)(cost | 1ull))) | (items << 6);
 }
 
 __global__ void k_item_classes(const BoxCells* __restrict__ bc, int nbox, int total, int npass, int* __restrict__ cls,
@@ -836,7 +850,7 @@ __global__ void k_item_classes(const BoxCells* __restrict__ bc, int nbox, int to
     const BoxCells box = bc[b];
     const int c = cell_items(box, g - box.base, npass);
     cls[g] = c;
-    if (c >= 0) atomicAdd(&sh[c & 63], c >> 6);
+    if (c >= 0 && (c >> 6) > 1) atomicAdd(&sh[c & 63], c >> 6);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kCostClasses; i += blockDim.x)
@@ -845,7 +859,7 @@ __global__ void k_item_classes(const BoxCells* __restrict__ bc, int nbox, int to
 
 // hist[0..63] -> start offsets, heaviest class first; nitems = total items.
 // One warp.
-__global__ void k_item_offsets(int* __restrict__ hist, int* __restrict__ start, int* __restrict__ nitems) {
+__global__ void k_item_offsets(int* __restrict__ hist, int* __restrict__ start, int* __restrict__ nitems, int total) {
   const int lane = threadIdx.x;
   // lane l owns classes 63 - 2l and 62 - 2l (descending order)
   const int a = hist[63 - 2 * lane], b = hist[62 - 2 * lane];
@@ -858,26 +872,39 @@ __global__ void k_item_offsets(int* __restrict__ hist, int* __restrict__ start, 
   const int excl = incl - a - b;
   start[63 - 2 * lane] = excl;
   start[62 - 2 * lane] = excl + a;
-  if (lane == 31) *nitems = incl;
+  if (lane == 31) {
+    nitems[0] = incl + total;  // split items, then one slot per cell
+    nitems[1] = incl;
+  }
   hist[63 - 2 * lane] = 0;  // reused as fill counters by the scatter
   hist[62 - 2 * lane] = 0;
 }
 
+// Split cells' pass items first, heaviest class first; then slot nsplit + g
+// for every cell g in natural (z, y, x) order -- the whole cell as one item,
+// or an empty marker (box -1) for empty, split or out-of-box cells -- so the
+// ordinary cells keep the spatial order of a per-cell launch.
 __global__ void k_item_scatter(const BoxCells* __restrict__ bc, int nbox, int total, const int* __restrict__ cls,
-                               const int* __restrict__ start, int* __restrict__ fill, int4* __restrict__ items) {
+                               const int* __restrict__ start, int* __restrict__ fill,
+                               const int* __restrict__ nitems, int4* __restrict__ items) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= total) return;
   const int c = cls[g];
-  if (c < 0) return;
+  const int nsplit = nitems[1];
+  if (c < 0) {
+    items[nsplit + g] = make_int4(-1, 0, 0, 0);
+    return;
+  }
   const int b = find_box(bc, nbox, g);
   const int key = g - __ldg(&bc[b].base);
   const int k = c >> 6, cl = c & 63;
-  const int at = start[cl] + atomicAdd(fill + cl, k);
   if (k == 1) {
-    items[at] = make_int4(b, key, 0, 0x7fffffff);
-  } else {
-    for (int p = 0; p < k; p++) items[at + p] = make_int4(b, key, p, p + 1);
+    items[nsplit + g] = make_int4(b, key, 0, 0x7fffffff);
+    return;
   }
+  items[nsplit + g] = make_int4(-1, 0, 0, 0);
+  const int at = start[cl] + atomicAdd(fill + cl, k);
+  for (int p = 0; p < k; p++) items[at + p] = make_int4(b, key, p, p + 1);
 }
 
 }  // namespace
@@ -1035,9 +1062,9 @@ int kick_batch_write_tables(tpm_ctx* const* boxes, int nbox, void* h_args, void*
     if (base > 0x7fffffffLL) return fail(TPM_ERR_INVALID, "batch has more than 2^31 chain cells");
   }
   *total_cells = base;
-  // a cell of n sinks gives one item, or ceil(n / npass) >= 2 items when
-  // n > npass >= 8: at most one item per cell plus one per 8 particles
-  *max_items = base + parts / 8 + nbox;
+  // one slot per cell, plus the pass items of split cells: a split cell of
+  // n sinks gives ceil(n / np) items with np >= 8, at most one per 8 particles
+  *max_items = 2 * base + parts / 8 + nbox;
   if (*max_items > 0x7fffffffLL) return fail(TPM_ERR_INVALID, "batch has more than 2^31 work items");
   return TPM_OK;
 }
@@ -1049,9 +1076,9 @@ int kick_batch_queue(const BatchQueue& q, int npass, cudaStream_t s) {
   const unsigned blocks = (unsigned)ceil_div(total, 256);
   k_item_classes<<<blocks, 256, 0, s>>>(static_cast<const BoxCells*>(q.d_cells), q.nbox, total, npass, q.d_class,
                                         q.d_hist);
-  k_item_offsets<<<1, 32, 0, s>>>(q.d_hist, q.d_hist + kCostClasses, q.d_nitems);
+  k_item_offsets<<<1, 32, 0, s>>>(q.d_hist, q.d_hist + kCostClasses, q.d_nitems, total);
   k_item_scatter<<<blocks, 256, 0, s>>>(static_cast<const BoxCells*>(q.d_cells), q.nbox, total, q.d_class,
-                                        q.d_hist + kCostClasses, q.d_hist, q.d_items);
+                                        q.d_hist + kCostClasses, q.d_hist, q.d_nitems, q.d_items);
   TPM_CUDA_TRY(cudaGetLastError());
   return TPM_OK;
 }
@@ -1064,12 +1091,13 @@ int kick_batch_interp(const BatchQueue& q, int min_rung, int npass, cudaStream_t
   return TPM_OK;
 }
 
-int kick_batch_kick(const BatchQueue& q, const KickShape& k, bool wrap, int min_rung, double scale, double t0,
-                    int first_call, cudaStream_t s, int* blocks_out) {
+int kick_batch_launch(const BatchQueue& q, const KickShape& k, bool wrap, int min_rung, double scale, double t0,
+                      int first_call, cudaStream_t s, int* blocks_out, const KickArgs* single) {
   if (!kick_shape_valid(k)) return fail(TPM_ERR_INVALID, "invalid kick shape");
   if (q.total_cells <= 0) return TPM_OK;
   const size_t smem = kick_smem(k);
-  auto kern = wrap ? k_kick_batch<true> : k_kick_batch<false>;
+  auto kern = single ? (wrap ? k_kick_batch<true, true> : k_kick_batch<false, true>)
+                     : (wrap ? k_kick_batch<true, false> : k_kick_batch<false, false>);
   TPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0, dev = 0, sms = 0;
   TPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * k.warps, smem));
@@ -1079,11 +1107,16 @@ int kick_batch_kick(const BatchQueue& q, const KickShape& k, bool wrap, int min_
   const int64_t blocks = std::min<int64_t>((int64_t)per_sm * sms, q.max_items);
   StepScalars st{min_rung, first_call ? 1 : 0, (float)t0, (float)scale};
   TPM_CUDA_TRY(cudaMemsetAsync(q.d_counter, 0, sizeof(int), s));
-  kern<<<(unsigned)blocks, 32 * k.warps, smem, s>>>(static_cast<const KickArgs*>(q.d_args), q.d_items, q.d_nitems,
-                                                    q.d_counter, st, k.stage, k.npass);
+  kern<<<(unsigned)blocks, 32 * k.warps, smem, s>>>(static_cast<const KickArgs*>(q.d_args), single ? *single : KickArgs{},
+                                                    q.d_items, q.d_nitems, q.d_counter, st, k.stage, k.npass);
   TPM_CUDA_TRY(cudaGetLastError());
   if (blocks_out) *blocks_out = (int)blocks;
   return TPM_OK;
+}
+
+int kick_batch_kick(const BatchQueue& q, const KickShape& k, bool wrap, int min_rung, double scale, double t0,
+                    int first_call, cudaStream_t s, int* blocks_out) {
+  return kick_batch_launch(q, k, wrap, min_rung, scale, t0, first_call, s, blocks_out, nullptr);
 }
 
 // The single-box kick through the same persistent queue: heavy cells split
@@ -1095,7 +1128,7 @@ int kick_queue_single(tpm_ctx* c, const KickArgs& a, const KickShape& k, int min
   if (!q.d_args) {
     q.nbox = 1;
     q.total_cells = ncell;
-    q.max_items = ncell + c->cap / 8 + 1;
+    q.max_items = 2 * ncell + c->cap / 8 + 1;
     if (q.max_items > 0x7fffffffLL) return fail(TPM_ERR_INVALID, "more than 2^31 work items");
     cudaError_t err = cudaMalloc(&q.d_args, sizeof(KickArgs));
     if (err == cudaSuccess) err = cudaMalloc(&q.d_cells, sizeof(BoxCells));
@@ -1126,7 +1159,7 @@ int kick_queue_single(tpm_ctx* c, const KickArgs& a, const KickShape& k, int min
   TPM_CUDA_TRY(cudaMemcpyAsync(q.d_args, ha, sizeof(KickArgs), cudaMemcpyHostToDevice, c->stream));
   TPM_CUDA_TRY(cudaMemcpyAsync(q.d_cells, hb, sizeof(BoxCells), cudaMemcpyHostToDevice, c->stream));
   int rc = kick_batch_queue(q, k.npass, c->stream);
-  if (rc == TPM_OK) rc = kick_batch_kick(q, k, c->C == 3, min_rung, scale, t0, first_call, c->stream, nullptr);
+  if (rc == TPM_OK) rc = kick_batch_launch(q, k, c->C == 3, min_rung, scale, t0, first_call, c->stream, nullptr, &a);
   c->launches += 4;
   return rc;
 }
