@@ -75,6 +75,9 @@ extern "C" {
  * else cuFFT; or cuFFT always. */
 #define TPM_FFT_AUTO 0
 #define TPM_FFT_CUFFT 1
+/* the library's transforms with the generic block engine for every mesh
+ * (AUTO takes the line engine where the mesh has a compiled line plan) */
+#define TPM_FFT_BLOCK 2
 
 typedef struct tpm_options {
   int four_dim;     /* PM grid points per side */

@@ -107,17 +107,34 @@ def test_force_at():
 
 
 # The library's own transforms (fft3d.cu) run for grids that are multiples of
-# 16 made of the radices 16, 8, 4, 3, 5 and 2 (48 = 16.3, 80 = 16.5,
-# 96 = 16.3.2, 128 = 16.8, 160 = 16.5.2); each is compared against both the
-# oracle and cuFFT on the same deposit.
+# 16 made of the radices 16, 8, 4, 3, 5 and 2: the generic block engine for
+# every such grid (fft="block"), the warp-per-line engine by default where the
+# grid has a compiled line plan (96, 128, 160 here; 48 and 80 have none and
+# take the block engine).  Each is compared against both the oracle and cuFFT
+# on the same deposit.
+@pytest.mark.parametrize("fft", ["auto", "block"])
 @pytest.mark.parametrize("grid", [48, 80, 96, 128, 160])
-def test_library_fft_matches_oracle_and_cufft(grid):
+def test_library_fft_matches_oracle_and_cufft(grid, fft):
     ps = particle_set("uniform", 20, 4)
     for typ in (GRAVITY_LONG_PME, GRAVITY_LONG_PM):
-        phi, (x, y, z) = device_phi(ps, grid, "cloud4", 2.0, typ, exact=True)
+        phi, (x, y, z) = device_phi(ps, grid, "cloud4", 2.0, typ, exact=True, fft=fft)
         phi_cu, _ = device_phi(ps, grid, "cloud4", 2.0, typ, exact=True, fft="cufft")
         ref = O.gravity_long(grid, 2.0, 0, x, y, z, pme=typ)
         assert rel_rms(phi, ref) < 2e-6, (grid, typ, rel_rms(phi, ref))
+        assert rel_rms(phi, phi_cu) < 2e-6, (grid, typ, rel_rms(phi, phi_cu))
+
+
+@pytest.mark.parametrize("grid", [64, 96, 128, 144, 160, 192, 240, 256, 288, 320, 384, 512, 576, 640])
+def test_line_fft_engine_matches_block_engine_and_cufft(grid):
+    """Every mesh with a compiled line plan (radix plans such as 12.8.8 at
+    768, 12.8.4 at 384, 12.12 at 144, 10.6.2.2 at 240) against the generic
+    block engine and cuFFT."""
+    ps = particle_set("uniform", 24, 6)
+    for typ in (GRAVITY_LONG_PME, GRAVITY_LONG_PM):
+        phi, _ = device_phi(ps, grid, "cloud4", 2.0, typ, exact=True)
+        phi_bl, _ = device_phi(ps, grid, "cloud4", 2.0, typ, exact=True, fft="block")
+        phi_cu, _ = device_phi(ps, grid, "cloud4", 2.0, typ, exact=True, fft="cufft")
+        assert rel_rms(phi, phi_bl) < 2e-6, (grid, typ, rel_rms(phi, phi_bl))
         assert rel_rms(phi, phi_cu) < 2e-6, (grid, typ, rel_rms(phi, phi_cu))
 
 

@@ -29,7 +29,7 @@ GRAVITY_LONG_PM = 0
 GRAVITY_LONG_PME = 1
 ASSIGN = {"cloud4": 0, "cic": 1, "tsc": 2}
 SORT = {"parity": 0, "fast": 1}
-FFT = {"auto": 0, "cufft": 1}
+FFT = {"auto": 0, "cufft": 1, "block": 2}
 
 
 class Options(C.Structure):

@@ -149,6 +149,74 @@ struct Dft<8, S> : DftSplit<8, S> {};
 template <int S>
 struct Dft<16, S> : DftSplit<16, S> {};
 
+// exp(S 2 pi i m / R) for R = 6, 10, 12 (m < R), as literals.
+template <int R>
+__device__ __forceinline__ float2 wtab(int m, int S) {
+  static_assert(R == 6 || R == 10 || R == 12, "composite radices 6, 10, 12");
+  constexpr float c6[6] = {1.0f, 0.5f, -0.5f, -1.0f, -0.5f, 0.5f};
+  constexpr float s6[6] = {0.0f, 0.86602540378443865f, 0.86602540378443865f, 0.0f, -0.86602540378443865f,
+                           -0.86602540378443865f};
+  constexpr float c10[10] = {1.0f, 0.80901699437494742f, 0.30901699437494742f, -0.30901699437494742f,
+                             -0.80901699437494742f, -1.0f, -0.80901699437494742f, -0.30901699437494742f,
+                             0.30901699437494742f, 0.80901699437494742f};
+  constexpr float s10[10] = {0.0f, 0.58778525229247313f, 0.95105651629515357f, 0.95105651629515357f,
+                             0.58778525229247313f, 0.0f, -0.58778525229247313f, -0.95105651629515357f,
+                             -0.95105651629515357f, -0.58778525229247313f};
+  constexpr float c12[12] = {1.0f, 0.86602540378443865f, 0.5f, 0.0f, -0.5f, -0.86602540378443865f,
+                             -1.0f, -0.86602540378443865f, -0.5f, 0.0f, 0.5f, 0.86602540378443865f};
+  constexpr float s12[12] = {0.0f, 0.5f, 0.86602540378443865f, 1.0f, 0.86602540378443865f, 0.5f,
+                             0.0f, -0.5f, -0.86602540378443865f, -1.0f, -0.86602540378443865f, -0.5f};
+  const float c = R == 6 ? c6[m] : (R == 10 ? c10[m] : c12[m]);
+  const float s = R == 6 ? s6[m] : (R == 10 ? s10[m] : s12[m]);
+  return make_float2(c, S > 0 ? s : -s);
+}
+
+// a * exp(S 2 pi i m / R), with the quarter turns as swaps and negations.
+template <int R, int S>
+__device__ __forceinline__ float2 twc(float2 a, int m) {
+  if (m == 0) return a;
+  if (4 * m == R) return imul<S>(a);
+  if (2 * m == R) return make_float2(-a.x, -a.y);
+  if (4 * m == 3 * R) return imul<-S>(a);
+  return cmul(a, wtab<R>(m, S));
+}
+
+// Composite R = A B point DFT (Cooley-Tukey in registers): with input index
+// m = a B + b and output index k = k1 + A k2,
+//   X[k1 + A k2] = sum_b w_B^(b k2) w_R^(b k1) sum_a v[a B + b] w_A^(a k1).
+template <int A, int B, int S>
+struct DftComp {
+  __device__ __forceinline__ static void run(float2* v) {
+    constexpr int R = A * B;
+    float2 t[R];
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      float2 u[A];
+#pragma unroll
+      for (int a = 0; a < A; a++) u[a] = v[a * B + b];
+      Dft<A, S>::run(u);
+#pragma unroll
+      for (int k1 = 0; k1 < A; k1++) t[b * A + k1] = twc<R, S>(u[k1], b * k1);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < A; k1++) {
+      float2 u[B];
+#pragma unroll
+      for (int b = 0; b < B; b++) u[b] = t[b * A + k1];
+      Dft<B, S>::run(u);
+#pragma unroll
+      for (int k2 = 0; k2 < B; k2++) v[k1 + A * k2] = u[k2];
+    }
+  }
+};
+
+template <int S>
+struct Dft<6, S> : DftComp<2, 3, S> {};
+template <int S>
+struct Dft<10, S> : DftComp<2, 5, S> {};
+template <int S>
+struct Dft<12, S> : DftComp<4, 3, S> {};
+
 // One Stockham stage of radix R over the block's lines of length N (line
 // stride LS), from shared buffer x to shared buffer y: butterfly j of a line
 // reads x[j + r N/R], applies the twiddles exp(S 2 pi i (j mod Ns) r / (Ns R)),
@@ -388,6 +456,469 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_z_c2r(const float2* __restr
   }
 }
 
+// ------------------------------------------------------------ line engine
+//
+// The same five passes for the mesh sizes that have a compile-time plan:
+// one line of length N is held by TL lanes of a warp (TL = 4 .. 32), E = N / TL
+// values per lane in registers.  A Stockham stage of radix R (R divides E)
+// gives every lane E / R butterflies j = lane + TL b; between stages the
+// line goes through its own row of shared memory with only warp-level
+// synchronisation, and the first stage reads its inputs (global rows, or the
+// block's transposed columns) and the last stage writes its outputs in
+// natural order straight from registers.  Radices, strides and divisions are
+// compile-time constants.  Column passes stage kLineCols = 8 neighbouring
+// columns per block (64-byte row segments) through shared memory.
+constexpr int kLineCols = 8;
+
+struct LinePlan {
+  int TL, E, ns;
+  int rad[6];
+};
+
+constexpr LinePlan line_plan_tl(int N, int TL) {
+  LinePlan p{TL, N / TL, 0, {1, 1, 1, 1, 1, 1}};
+  if (N % TL != 0) {
+    p.ns = 99;
+    return p;
+  }
+  constexpr int cand[9] = {16, 12, 10, 8, 6, 5, 4, 3, 2};
+  int M = N;
+  while (M > 1) {
+    int pick = 0;
+    for (int i = 0; i < 9; i++)
+      if (pick == 0 && p.E % cand[i] == 0 && M % cand[i] == 0) pick = cand[i];
+    if (pick == 0 || p.ns == 6) {
+      p.ns = 99;
+      return p;
+    }
+    p.rad[p.ns++] = pick;
+    M /= pick;
+  }
+  return p;
+}
+
+// Fewest stages with at most 36 values per lane; ties go to more lanes per line.
+constexpr LinePlan line_plan(int N) {
+  LinePlan best{0, 0, 99, {1, 1, 1, 1, 1, 1}};
+  constexpr int tls[4] = {32, 16, 8, 4};
+  for (int i = 0; i < 4; i++) {
+    const LinePlan p = line_plan_tl(N, tls[i]);
+    if (p.ns < 99 && p.E <= 36 && p.ns < best.ns) best = p;
+  }
+  return best;
+}
+
+constexpr int ns_before(const LinePlan& p, int st) {
+  int r = 1;
+  for (int i = 0; i < st; i++) r *= p.rad[i];
+  return r;
+}
+
+// The same radices in the opposite order.  A transform with the reversed plan
+// takes its first-stage inputs in exactly the registers where the forward
+// plan's last stage leaves its outputs (lane + TL b + r N / R_last).
+constexpr LinePlan reverse_plan(const LinePlan& p) {
+  LinePlan q = p;
+  for (int i = 0; i < p.ns; i++) q.rad[i] = p.rad[p.ns - 1 - i];
+  return q;
+}
+
+template <int N>
+struct LineCfg {
+  static constexpr LinePlan P = line_plan(N);
+  static constexpr int TL = P.TL, E = P.E;
+  static constexpr int kThreads = kLineCols * TL;
+  // line stride = N + 4 (N % 16 == 0): the transposed column loads of 8
+  // columns x 4 rows per warp then fall in distinct bank pairs
+  static constexpr int LS = N + 4;
+  // resident threads per SM the register budget targets: 768 (85 registers),
+  // 512 (128 registers) from 28 values per lane up
+  static constexpr int kMinBlocks = (E >= 28 ? 2 : 3) * 256 / kThreads;
+  static constexpr size_t kSmem = sizeof(float2) * ((size_t)N + (size_t)kLineCols * LS);
+  // the x pass holds the stage tables of both radix orders
+  static constexpr size_t kSmemX = kSmem + sizeof(float2) * (size_t)N;
+  static_assert(P.ns >= 1 && P.ns <= 6, "no line plan for this N");
+};
+
+// One line transform of sign S with the plan of N (REV: its radices reversed).
+template <int N, int S, bool REV = false>
+struct LineFft {
+  using L = LineCfg<N>;
+  static constexpr LinePlan P = REV ? reverse_plan(L::P) : L::P;
+  static constexpr int TL = L::TL, E = L::E;
+  // butterfly stride of the last stage: output r of butterfly j is j + r NL
+  static constexpr int NL = N / P.rad[P.ns - 1];
+
+  // Stage ST: v holds its inputs, v[b R + r] = x[j + r N / R] for the lane's
+  // butterflies j = lane + TL b; twiddles exp(S 2 pi i (j mod Ns) r / (Ns R))
+  // from the stage table (line_twiddle_table): entry Ns - 1 + k (R - 1) + r - 1
+  // holds exp(-2 pi i k r / (Ns R)), so the R - 1 twiddles of one butterfly
+  // are contiguous and the lanes' reads stride by R - 1 values.
+  template <int ST, class Out>
+  __device__ __forceinline__ static void stage(float2* __restrict__ line, float2 (&v)[E],
+                                               const float2* __restrict__ tw, int lane, Out& out) {
+    constexpr int R = P.rad[ST];
+    constexpr int NS = ns_before(P, ST);
+    constexpr int NB = E / R;
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      if (NS > 1) {
+        const int j = lane + TL * b;
+        const float2* tws = tw + (NS - 1) + (j % NS) * (R - 1);
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+          float2 w = tws[r - 1];
+          if (S > 0) w.y = -w.y;
+          v[b * R + r] = cmul(v[b * R + r], w);
+        }
+      }
+      Dft<R, S>::run(v + b * R);
+    }
+    if constexpr (ST == P.ns - 1) {
+      // Ns R = N: butterfly j's outputs are x[j + r Ns], natural order
+#pragma unroll
+      for (int b = 0; b < NB; b++)
+#pragma unroll
+        for (int r = 0; r < R; r++) out(lane + TL * b + r * NS, v[b * R + r]);
+    } else {
+      if (NS == 1 && R % 2 == 0) {
+        // first stage: butterfly j's R outputs are contiguous (x[j R + r]);
+        // 16-byte stores of two values each (a lane stride of R values would
+        // put 8 or 16 lanes of a scalar store on one bank pair)
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+          float4* dst = reinterpret_cast<float4*>(line + (lane + TL * b) * R);
+#pragma unroll
+          for (int r = 0; r < R; r += 2)
+            dst[r / 2] = make_float4(v[b * R + r].x, v[b * R + r].y, v[b * R + r + 1].x, v[b * R + r + 1].y);
+        }
+      } else {
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+          const int j = lane + TL * b;
+          const int q = j / NS, k = j - q * NS;
+#pragma unroll
+          for (int r = 0; r < R; r++) line[q * NS * R + k + r * NS] = v[b * R + r];
+        }
+      }
+      __syncwarp();
+      constexpr int R2 = P.rad[ST + 1];
+#pragma unroll
+      for (int b = 0; b < E / R2; b++)
+#pragma unroll
+        for (int r = 0; r < R2; r++) v[b * R2 + r] = line[lane + TL * b + r * (N / R2)];
+      __syncwarp();
+      stage<ST + 1>(line, v, tw, lane, out);
+    }
+  }
+
+  // First-stage inputs into v: v[b R + r] = in(lane + TL b + r N / R).
+  template <class In>
+  __device__ __forceinline__ static void load(float2 (&v)[E], int lane, In in) {
+    constexpr int R = P.rad[0];
+#pragma unroll
+    for (int b = 0; b < E / R; b++)
+#pragma unroll
+      for (int r = 0; r < R; r++) v[b * R + r] = in(lane + TL * b + r * (N / R));
+  }
+
+  // The transform from inputs already in v (as load leaves them); out(n, value)
+  // takes output n, and v keeps the outputs, v[b R + r] = X[lane + TL b + r NL].
+  template <class Out>
+  __device__ __forceinline__ static void from_regs(float2* __restrict__ line, float2 (&v)[E],
+                                                   const float2* __restrict__ tw, int lane, Out out) {
+    stage<0>(line, v, tw, lane, out);
+  }
+
+  // Transform of one line: in(n) gives input n, out(n, value) takes output n.
+  // line is the line's shared-memory row (TL lanes); in may read it.
+  template <class In, class Out>
+  __device__ __forceinline__ static void run(float2* __restrict__ line, const float2* __restrict__ tw, int lane,
+                                             In in, Out out) {
+    float2 v[E];
+    load(v, lane, in);
+    __syncwarp();
+    stage<0>(line, v, tw, lane, out);
+  }
+};
+
+template <int N>
+__device__ __forceinline__ void line_twiddles(float2* s_tw, const float2* __restrict__ tw) {
+  for (int i = threadIdx.x; i < N; i += LineCfg<N>::kThreads) s_tw[i] = __ldg(tw + i);
+}
+
+// Load / store the block's kLineCols columns (rows y < N at stride rs) into /
+// from the transposed shared-memory lines, two columns per 16-byte access.
+// Every load is issued before the first shared store (E / 2 loads in flight
+// per thread).
+template <int N>
+__device__ __forceinline__ void cols_load(float2* __restrict__ lines, const float2* __restrict__ g, int64_t rs) {
+  using L = LineCfg<N>;
+  constexpr int IT = (kLineCols / 2) * N / L::kThreads;
+  static_assert(IT * L::kThreads == (kLineCols / 2) * N, "column tile per thread");
+  float4 u[IT];
+#pragma unroll
+  for (int i = 0; i < IT; i++) {
+    const int e = threadIdx.x + i * L::kThreads;
+    const int y = e / (kLineCols / 2), c = 2 * (e - y * (kLineCols / 2));
+    u[i] = __ldg(reinterpret_cast<const float4*>(g + y * rs + c));
+  }
+#pragma unroll
+  for (int i = 0; i < IT; i++) {
+    const int e = threadIdx.x + i * L::kThreads;
+    const int y = e / (kLineCols / 2), c = 2 * (e - y * (kLineCols / 2));
+    lines[c * L::LS + y] = make_float2(u[i].x, u[i].y);
+    lines[(c + 1) * L::LS + y] = make_float2(u[i].z, u[i].w);
+  }
+}
+template <int N>
+__device__ __forceinline__ void cols_store(const float2* __restrict__ lines, float2* __restrict__ g, int64_t rs) {
+  using L = LineCfg<N>;
+  constexpr int IT = (kLineCols / 2) * N / L::kThreads;
+  // thread index through an opaque move: the load's address arithmetic is
+  // then recomputed here instead of being kept live across the transform
+  int t;
+  asm volatile("mov.b32 %0, %1;" : "=r"(t) : "r"((int)threadIdx.x));
+#pragma unroll
+  for (int i = 0; i < IT; i++) {
+    const int e = t + i * L::kThreads;
+    const int y = e / (kLineCols / 2), c = 2 * (e - y * (kLineCols / 2));
+    const float2 a = lines[c * L::LS + y], b = lines[(c + 1) * L::LS + y];
+    *reinterpret_cast<float4*>(g + y * rs + c) = make_float4(a.x, a.y, b.x, b.y);
+  }
+}
+
+// P1 (line engine): rows (x, 2p), (x, 2p+1) as one complex line, forward z
+// transform, the two half-spectra separated into spectrum rows 2p, 2p+1.
+template <int N>
+__global__ void __launch_bounds__(LineCfg<N>::kThreads, LineCfg<N>::kMinBlocks)
+    k_line_z_r2c(const float* __restrict__ rho, float2* __restrict__ Y, int Sz, const float2* __restrict__ tw,
+                 int x0) {
+  using L = LineCfg<N>;
+  extern __shared__ __align__(16) float2 lsm[];
+  float2* s_tw = lsm;
+  line_twiddles<N>(s_tw, tw);
+  const int li = threadIdx.x / L::TL, lane = threadIdx.x - li * L::TL;
+  float2* line = lsm + N + li * L::LS;
+  constexpr int per_x = N / (2 * kLineCols);
+  const int xb = blockIdx.x / per_x;
+  const int p = (blockIdx.x - xb * per_x) * kLineCols + li;
+  const int64_t row = (int64_t)(x0 + xb) * N + 2 * p;
+  const float* r0 = rho + row * N;
+  const float* r1 = r0 + N;
+  __syncthreads();
+  LineFft<N, -1>::run(
+      line, s_tw, lane, [&](int n) { return make_float2(__ldg(r0 + n), __ldg(r1 + n)); },
+      [&](int n, float2 v) { line[n] = v; });
+  __syncwarp();
+  float2* y0 = Y + row * Sz;
+  float2* y1 = y0 + Sz;
+  constexpr int Nh = N / 2 + 1;
+  for (int kz = lane; kz < Sz; kz += L::TL) {
+    float2 a = make_float2(0.f, 0.f), b = a;  // padding columns stay zero
+    if (kz < Nh) {
+      const float2 zk = line[kz];
+      const float2 zm = line[kz == 0 ? 0 : N - kz];
+      a = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+      b = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    }
+    y0[kz] = a;
+    y1[kz] = b;
+  }
+}
+
+// P2 / P4 (line engine): the 8 columns [c0, c0 + 8) of plane x along y.
+template <int N, int S>
+__global__ void __launch_bounds__(LineCfg<N>::kThreads, LineCfg<N>::kMinBlocks)
+    k_line_y(float2* __restrict__ Y, int Sz, const float2* __restrict__ tw, int x0) {
+  using L = LineCfg<N>;
+  extern __shared__ __align__(16) float2 lsm[];
+  float2* s_tw = lsm;
+  float2* lines = lsm + N;
+  line_twiddles<N>(s_tw, tw);
+  const int li = threadIdx.x / L::TL, lane = threadIdx.x - li * L::TL;
+  float2* line = lines + li * L::LS;
+  const int per_x = Sz / kLineCols;
+  const int xb = blockIdx.x / per_x;
+  const int c0 = (blockIdx.x - xb * per_x) * kLineCols;
+  float2* plane = Y + (int64_t)(x0 + xb) * N * Sz + c0;
+  cols_load<N>(lines, plane, Sz);
+  __syncthreads();
+  LineFft<N, S>::run(
+      line, s_tw, lane, [&](int n) { return line[n]; }, [&](int n, float2 v) { line[n] = v; });
+  __syncthreads();
+  cols_store<N>(lines, plane, Sz);
+}
+
+// P3 (line engine): the 8 columns [c0, c0 + 8) of row y along x: forward
+// transform, Green's function (as k_fft_x_green), inverse transform.  The
+// inverse runs the reversed radix plan, so it starts from the registers the
+// forward transform ends in, with the Green's function applied there: the
+// spectrum of the line does not go through shared memory between the two.
+// tw: the forward plan's stage tables, then the reversed plan's (N each).
+template <int N>
+__global__ void __launch_bounds__(LineCfg<N>::kThreads, LineCfg<N>::kMinBlocks)
+    k_line_x_green(float2* __restrict__ Y, int Sz, const float2* __restrict__ tw, const float* __restrict__ gt,
+                   const float* __restrict__ k2tab, float norm) {
+  using L = LineCfg<N>;
+  using Fwd = LineFft<N, -1, false>;
+  using Inv = LineFft<N, 1, true>;
+  extern __shared__ __align__(16) float2 lsm[];
+  float2* s_tw = lsm;
+  float2* s_twr = lsm + N;
+  float2* lines = lsm + 2 * N;
+  for (int i = threadIdx.x; i < 2 * N; i += L::kThreads) s_tw[i] = __ldg(tw + i);
+  const int li = threadIdx.x / L::TL, lane = threadIdx.x - li * L::TL;
+  float2* line = lines + li * L::LS;
+  const int per_y = Sz / kLineCols;
+  const int y = blockIdx.x / per_y;
+  const int c0 = (blockIdx.x - y * per_y) * kLineCols;
+  float2* col = Y + (int64_t)y * Sz + c0;
+  const int64_t xs = (int64_t)N * Sz;
+  cols_load<N>(lines, col, xs);
+  __syncthreads();
+  const int kz = c0 + li;
+  const bool live = kz < N / 2 + 1;
+  const float k2yz = __ldg(k2tab + y) + (live ? __ldg(k2tab + kz) : 0.f);
+  const float gyz = __ldg(gt + y) * (live ? __ldg(gt + kz) : 0.f);
+  float2 v[L::E];
+  Fwd::load(v, lane, [&](int n) { return line[n]; });
+  __syncwarp();
+  Fwd::from_regs(line, v, s_tw, lane, [](int, float2) {});
+  // v[b R + r] = X[lane + TL b + r NL]: the Green's function in registers
+  constexpr int RL = Fwd::P.rad[Fwd::P.ns - 1];
+#pragma unroll
+  for (int b = 0; b < L::E / RL; b++)
+#pragma unroll
+    for (int r = 0; r < RL; r++) {
+      const int n = lane + L::TL * b + r * Fwd::NL;
+      const float k2 = __ldg(k2tab + n) + k2yz;
+      const float g = k2 > 0.0f ? -(__ldg(gt + n) * gyz) * __frcp_rn(k2) * norm : 0.0f;
+      v[b * RL + r] = make_float2(v[b * RL + r].x * g, v[b * RL + r].y * g);
+    }
+  // The inverse recomputes its addresses: with the lane index passed through
+  // an opaque move, the forward transform's index arithmetic is not kept
+  // live across the inverse (it would spill).
+  int lane2;
+  asm volatile("mov.b32 %0, %1;" : "=r"(lane2) : "r"(lane));
+  Inv::from_regs(line, v, s_twr, lane2, [&](int n, float2 u) { line[n] = u; });
+  __syncthreads();
+  cols_store<N>(lines, col, xs);
+}
+
+// P5 (line engine): spectrum rows 2p, 2p+1 recombined (Z = A + i B, the
+// Hermitian halves mirrored), inverse z transform, real -> row 2p, imag -> 2p+1.
+template <int N>
+__global__ void __launch_bounds__(LineCfg<N>::kThreads, LineCfg<N>::kMinBlocks)
+    k_line_z_c2r(const float2* __restrict__ Y, float* __restrict__ phi, int Sz, const float2* __restrict__ tw,
+                 int x0) {
+  using L = LineCfg<N>;
+  extern __shared__ __align__(16) float2 lsm[];
+  float2* s_tw = lsm;
+  line_twiddles<N>(s_tw, tw);
+  const int li = threadIdx.x / L::TL, lane = threadIdx.x - li * L::TL;
+  float2* line = lsm + N + li * L::LS;
+  constexpr int per_x = N / (2 * kLineCols);
+  const int xb = blockIdx.x / per_x;
+  const int p = (blockIdx.x - xb * per_x) * kLineCols + li;
+  const int64_t row = (int64_t)(x0 + xb) * N + 2 * p;
+  const float2* y0 = Y + row * Sz;
+  const float2* y1 = y0 + Sz;
+  float* f0 = phi + row * N;
+  float* f1 = f0 + N;
+  __syncthreads();
+  LineFft<N, 1>::run(
+      line, s_tw, lane,
+      [&](int n) {
+        float2 a, b;
+        if (n <= N / 2) {
+          a = __ldg(y0 + n);
+          b = __ldg(y1 + n);
+          if (n == 0 || n == N / 2) {
+            a.y = 0.0f;
+            b.y = 0.0f;
+          }
+        } else {
+          a = __ldg(y0 + (N - n));
+          b = __ldg(y1 + (N - n));
+          a.y = -a.y;
+          b.y = -b.y;
+        }
+        return make_float2(a.x - b.y, a.y + b.x);
+      },
+      [&](int n, float2 v) {
+        f0[n] = v.x;
+        f1[n] = v.y;
+      });
+}
+
+template <int N>
+int line_set_smem() {
+  using L = LineCfg<N>;
+  const int s = (int)L::kSmem;
+  TPM_CUDA_TRY(cudaFuncSetAttribute(k_line_z_r2c<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+  TPM_CUDA_TRY(cudaFuncSetAttribute(k_line_y<N, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+  TPM_CUDA_TRY(cudaFuncSetAttribute(k_line_y<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+  TPM_CUDA_TRY(
+      cudaFuncSetAttribute(k_line_x_green<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::kSmemX));
+  TPM_CUDA_TRY(cudaFuncSetAttribute(k_line_z_c2r<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+  return TPM_OK;
+}
+
+template <int N>
+int line_poisson(tpm_ctx* c, float2* Y, int Sz, const float* gt, float norm) {
+  using L = LineCfg<N>;
+  // the kernels' shared-memory size depends on N alone: set once per N
+  static const int attr = line_set_smem<N>();
+  if (attr) return attr;
+  cudaStream_t s = c->stream;
+  const unsigned zblocks = (unsigned)(N * (N / (2 * kLineCols)));
+  const unsigned cblocks = (unsigned)(N * (Sz / kLineCols));
+  const float2* tw = c->fft_tw + N;  // the stage tables of the line plan, then of its reversal
+  stage_begin(c, kStFftF);
+  k_line_z_r2c<N><<<zblocks, L::kThreads, L::kSmem, s>>>(c->rho, Y, Sz, tw, 0);
+  k_line_y<N, -1><<<cblocks, L::kThreads, L::kSmem, s>>>(Y, Sz, tw, 0);
+  stage_end(c, kStFftF);
+  stage_begin(c, kStGreen);
+  k_line_x_green<N><<<cblocks, L::kThreads, L::kSmemX, s>>>(Y, Sz, tw, gt, c->k2tab, norm);
+  stage_end(c, kStGreen);
+  stage_begin(c, kStFftI);
+  k_line_y<N, 1><<<cblocks, L::kThreads, L::kSmem, s>>>(Y, Sz, tw, 0);
+  k_line_z_c2r<N><<<zblocks, L::kThreads, L::kSmem, s>>>(Y, c->phi, Sz, tw, 0);
+  stage_end(c, kStFftI);
+  c->launches += 5;
+  TPM_CUDA_TRY(cudaGetLastError());
+  return TPM_OK;
+}
+
+// Mesh sizes with a compiled line plan (the benchmark meshes, the batched
+// and served box meshes, and the powers of two up to 1024).
+#define TPM_LINE_SIZES(X) \
+  X(64) X(96) X(128) X(144) X(160) X(192) X(240) X(256) X(288) X(320) X(384) X(512) X(576) X(640) X(768) X(1024)
+
+bool line_supported(int N) {
+  switch (N) {
+#define TPM_LINE_CASE(n) case n:
+    TPM_LINE_SIZES(TPM_LINE_CASE)
+#undef TPM_LINE_CASE
+    return true;
+    default:
+      return false;
+  }
+}
+
+int line_dispatch(tpm_ctx* c, float2* Y, int Sz, const float* gt, float norm) {
+  switch (c->N) {
+#define TPM_LINE_CASE(n) \
+  case n:                \
+    return line_poisson<n>(c, Y, Sz, gt, norm);
+    TPM_LINE_SIZES(TPM_LINE_CASE)
+#undef TPM_LINE_CASE
+    default:
+      return fail(TPM_ERR_INVALID, "fft3d: no line plan for this mesh");
+  }
+}
+
 bool plan_radices(int N, FftPlan& p) {
   p.N = N;
   p.nrad = 0;
@@ -433,7 +964,7 @@ int plane_group(const tpm_ctx* c, int N) {
 
 }  // namespace
 
-int fft3d_padded_columns(int N) { return ((N / 2 + 1) + kFftLines - 1) / kFftLines * kFftLines; }
+int fft3d_padded_columns(int N) { return ((N / 2 + 1) + kLineCols - 1) / kLineCols * kLineCols; }
 
 bool fft3d_supported(int N) {
   FftPlan p;
@@ -442,12 +973,34 @@ bool fft3d_supported(int N) {
 
 int fft3d_init(tpm_ctx* c) {
   const int N = c->N;
-  std::vector<float2> tw(N);
+  // [0, N): exp(-2 pi i m / N) for the block engine; [N, 2N) and [2N, 3N):
+  // the line engine's stage tables of its plan and of the reversed plan,
+  // entry Ns - 1 + k (R - 1) + r - 1 of a stage of radix R after Ns points =
+  // exp(-2 pi i k r / (Ns R)), k < Ns, 0 < r < R (the stages' Ns (R - 1)
+  // entries add up to N - 1).  All in FP64.
+  std::vector<float2> tw(3 * (size_t)N, make_float2(0.f, 0.f));
   for (int m = 0; m < N; m++) {
     const double a = -2.0 * M_PI * (double)m / (double)N;
     tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
   }
-  TPM_CUDA_TRY(cudaMemcpy(c->fft_tw, tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
+  if (line_supported(N)) {
+    const LinePlan plans[2] = {line_plan(N), reverse_plan(line_plan(N))};
+    for (int pi = 0; pi < 2; pi++) {
+      const LinePlan& P = plans[pi];
+      float2* t = tw.data() + (size_t)(pi + 1) * N;
+      int ns = 1;
+      for (int s = 0; s < P.ns; s++) {
+        const int R = P.rad[s];
+        for (int k = 0; k < ns; k++)
+          for (int r = 1; r < R; r++) {
+            const double a = -2.0 * M_PI * (double)k * r / ((double)ns * R);
+            t[ns - 1 + k * (R - 1) + r - 1] = make_float2((float)std::cos(a), (float)std::sin(a));
+          }
+        ns *= R;
+      }
+    }
+  }
+  TPM_CUDA_TRY(cudaMemcpy(c->fft_tw, tw.data(), sizeof(float2) * 3 * N, cudaMemcpyHostToDevice));
   // padding columns stay zero: the transforms keep them zero and never store them into phi
   if (c->rhok) TPM_CUDA_TRY(cudaMemset(c->rhok, 0, sizeof(float2) * (size_t)N * N * fft3d_padded_columns(N)));
   const int smem = (int)fft_smem(N);
@@ -460,13 +1013,14 @@ int fft3d_poisson(tpm_ctx* c, const float* gt) {
   plan_radices(N, p);
   p.Sz = fft3d_padded_columns(N);
   float2* Y = reinterpret_cast<float2*>(c->rhok);
+  const float norm = (float)(1.0 / ((double)N * N * N));
+  if (c->opt.fft != TPM_FFT_BLOCK && line_supported(N)) return line_dispatch(c, Y, p.Sz, gt, norm);
   const size_t smem = fft_smem(N);
   const int rca = set_fft_smem(smem);
   if (rca) return rca;
   cudaStream_t s = c->stream;
   const unsigned zblocks = (unsigned)(N * (N / (2 * kFftLines)));
   const unsigned cblocks = (unsigned)(N * (p.Sz / kFftLines));
-  const float norm = (float)(1.0 / ((double)N * N * N));
   stage_begin(c, kStFftF);
   // The z and y passes work plane by plane in x: launched a group of planes
   // at a time, the spectrum one z pass writes is still in L2 when the y pass

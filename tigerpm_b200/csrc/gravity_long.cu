@@ -107,7 +107,13 @@ struct DepAcc<true> {
 template <>
 struct DepAcc<false> {
   using T = float;
+#ifdef TPM_DEP_RED
+  static __device__ __forceinline__ void add(T* p, float w) {
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "f"(w) : "memory");
+  }
+#else
   static __device__ __forceinline__ void add(T* p, float w) { atomicAdd(p, w); }
+#endif
   static __device__ __forceinline__ double value(T v, double scale) { return (double)v * scale; }
 };
 

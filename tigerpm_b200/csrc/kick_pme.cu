@@ -227,7 +227,12 @@ __device__ __forceinline__ void interp_cell_direct(const KickArgs& a, int64_t ke
   }
 }
 
-__global__ void __launch_bounds__(64) k_interp_direct(KickArgs a) {
+// 12 resident 64-thread blocks per SM (at most 85 registers): 2.55 ms against
+// 2.78 ms with the compiler's own choice at 256^3 on a 768^3 mesh
+#ifndef TPM_INTERP_MINB
+#define TPM_INTERP_MINB 12
+#endif
+__global__ void __launch_bounds__(64, TPM_INTERP_MINB) k_interp_direct(KickArgs a) {
   int bid = blockIdx.x;
   const int i2 = bid % a.s2;
   bid /= a.s2;
@@ -374,7 +379,9 @@ __device__ __forceinline__ void pair(const PairK& k, float dx, float dy, float d
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   // Pairs beyond the cutoff take r^2 = 1e30: 1/r, erfc and exp(-x^2) then
   // vanish and the pair adds exactly 0, without a mask on the results.
-  const float r2c = r2 < k.rcut2 ? fmaxf(r2, k.h2) : 1e30f;
+  // Pairs at r <= h (the sink itself included, r = 0) take the softened
+  // branch below, which replaces every term the lines before it form.
+  const float r2c = r2 < k.rcut2 ? r2 : 1e30f;
   const float rinv = rsqrt_approx(r2c);
   const float r = r2c * rinv;
   // A&S 7.1.26 erfc(x0) with x0 = r; exp(-x0^2) = 2^(-log2(e) r^2)
@@ -382,22 +389,20 @@ __device__ __forceinline__ void pair(const PairK& k, float dx, float dy, float d
   const float e = ex2_approx(-1.4426950408889634f * r2c);
   const float poly =
       t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f), 0.254829592f);
-  const float erfc0 = poly * e;
-  const float rinv2 = rinv * rinv;
-  float rinv3 = fmaf(1.1283791670955126f * r, e, erfc0) * rinv2 * rinv;  // 2/sqrt(pi)
-  float rinv1 = erfc0;  // times 1/r below
-  float rscale = rinv;
+  // potential term erfc / r, and the force term
+  // (erfc + (2/sqrt(pi)) r e) / r^3 = (erfc / r + (2/sqrt(pi)) e) / r^2
+  float q = poly * e * rinv;
+  float rinv3 = fmaf(1.1283791670955126f, e, q) * (rinv * rinv);
   if (r2 <= k.h2) {  // softened Newtonian kernel inside hsoft (rare)
     const float hinv = rsqrtf(k.h2);
     const float q2 = r2 * hinv * hinv;
     rinv3 = fmaf(fmaf(15.0f / 8.0f, q2, -21.0f / 4.0f), q2, 35.0f / 8.0f) * (hinv * hinv * hinv);
-    rinv1 = fmaf(fmaf(fmaf(-5.0f / 16.0f, q2, 21.0f / 16.0f), q2, -35.0f / 16.0f), q2, 35.0f / 16.0f);
-    rscale = hinv;
+    q = fmaf(fmaf(fmaf(-5.0f / 16.0f, q2, 21.0f / 16.0f), q2, -35.0f / 16.0f), q2, 35.0f / 16.0f) * hinv;
   }
   gx = fmaf(-dx, rinv3, gx);
   gy = fmaf(-dy, rinv3, gy);
   gz = fmaf(-dz, rinv3, gz);
-  ph = fmaf(-rinv1, rscale, ph);
+  ph -= q;
 }
 
 // Offset a - b of two fixed32 coordinates (the reference's int32 wrap-around

@@ -65,7 +65,7 @@ int64_t plan_bytes(const tpm_options& o, int64_t cap) {
   b += 4 * (2 * ((cap + T - 1) / T + (ncell + T - 1) / T) + 64);  // blocksums
   b += 8 * ((std::max(cap, ncell) + T - 1) / T + 1);  // look-back status words
   b += 8 * (ncell + 2);                        // counts + offsets
-  b += N * N * N * 4 * 2 + N * N * (int64_t)fft3d_padded_columns((int)N) * 8 + N * 8;  // rho, phi, rhok, twiddles
+  b += N * N * N * 4 * 2 + N * N * (int64_t)fft3d_padded_columns((int)N) * 8 + 3 * N * 8;  // rho, phi, rhok, twiddles
   return b;
 }
 
@@ -77,7 +77,7 @@ int derive(tpm_ctx* c) {
   if (!(o.rs > 0) || !(o.hsoft > 0)) return fail(TPM_ERR_INVALID, "rs and hsoft must be positive");
   if (o.assign < 0 || o.assign > 2) return fail(TPM_ERR_INVALID, "assign must be cloud4, cic or tsc");
   if (o.sort_mode < 0 || o.sort_mode > 1) return fail(TPM_ERR_INVALID, "sort_mode must be parity or fast");
-  if (o.fft < 0 || o.fft > 1) return fail(TPM_ERR_INVALID, "fft must be auto or cufft");
+  if (o.fft < 0 || o.fft > 2) return fail(TPM_ERR_INVALID, "fft must be auto, cufft or block");
   c->N = o.four_dim;
   c->C = o.chain_dim;
   c->rs_box = o.rs;
@@ -200,6 +200,7 @@ int tpm_options_parse(tpm_options* o, int argc, const char* const* argv) {
     } else if (key == "fft") {
       if (val == "auto") fft = TPM_FFT_AUTO;
       else if (val == "cufft") fft = TPM_FFT_CUFFT;
+      else if (val == "block") fft = TPM_FFT_BLOCK;
       else ok = false;
     } else return fail(TPM_ERR_INVALID, "unknown option --" + key);
     if (!ok) return fail(TPM_ERR_INVALID, "bad value for --" + key + ": " + val);
@@ -353,7 +354,7 @@ int tpm::ctx_create(const tpm_options* opts, int64_t capacity, bool with_scratch
   A.get(c->thr, C + 1);
   A.get(c->tree, C * kMaxTreeDepth);
   A.get(c->depth1d, C);
-  A.get(c->fft_tw, N);
+  A.get(c->fft_tw, 3 * N);
   A.get(c->gtab, 2 * N);
   A.get(c->k2tab, N);
   A.get(c->d_err, 1);

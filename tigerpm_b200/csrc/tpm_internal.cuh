@@ -118,7 +118,7 @@ struct tpm_ctx {
   // mesh
   float* rho = nullptr;  // N^3 real grid (deposit out, r2c in)
   cufftComplex* rhok = nullptr;  // N x N x Sz spectrum (Sz = N/2+1 rounded up to 8)
-  float2* fft_tw = nullptr;       // exp(-2 pi i m / N), m < N, for the library's own transforms
+  float2* fft_tw = nullptr;       // 3N twiddles of the library's own transforms (fft3d_init)
   bool use_fft3d = false;         // library transforms instead of cuFFT
   float* phi = nullptr;  // N^3
   float* gtab = nullptr;   // exp(-k^2 rs^2) sinc(k/2)^-p per index, N
