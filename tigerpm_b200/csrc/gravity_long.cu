@@ -107,22 +107,73 @@ struct DepAcc<true> {
 template <>
 struct DepAcc<false> {
   using T = float;
-#ifdef TPM_DEP_RED
-  static __device__ __forceinline__ void add(T* p, float w) {
-    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "f"(w) : "memory");
-  }
-#else
   static __device__ __forceinline__ void add(T* p, float w) { atomicAdd(p, w); }
-#endif
   static __device__ __forceinline__ double value(T v, double scale) { return (double)v * scale; }
 };
 
+// The candidates of a tile (the particles of the chain cells that can reach
+// it: 9 to 16 rows of 3 to 4 x cells, up to twice 8x the tile's own) are one
+// flat index space over at most kDepRuns contiguous runs; each thread loads
+// kDepBatch candidates at a time (independent loads in flight), and the
+// reaching ones are compacted into a shared list of up to kDepList particle
+// indices before they are deposited, so that every thread of the block
+// deposits an equal share.
+constexpr int kDepThreads = 256;
+constexpr int kDepBatch = 4;
+constexpr int kDepList = 2048;
+constexpr int kDepRuns = 64;
+
+// Weights of one particle added to the tile (stencil origin o, extent ext).
 template <int T, int ASSIGN, bool EXACT>
-__global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
+__device__ __forceinline__ void deposit_particle(typename DepAcc<EXACT>::T* acc, int4 q, int N, const int (&o)[3],
+                                                 const int (&ext)[3]) {
+  constexpr int W = Width<ASSIGN>::W;
+  using A = DepAcc<EXACT>;
+  float wx[4], wy[4], wz[4];
+  int r[3];
+  r[0] = stencil<ASSIGN>((uint32_t)q.x, N, wx) - o[0];
+  r[1] = stencil<ASSIGN>((uint32_t)q.y, N, wy) - o[1];
+  r[2] = stencil<ASSIGN>((uint32_t)q.z, N, wz) - o[2];
+  int li[3][4];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+      int l = r[d] + k;
+      if (l < 0) l += N;
+      else if (l >= N) l -= N;
+      li[d][k] = l < ext[d] ? l : -1;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < W; i++) {
+    if (li[0][i] < 0) continue;
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      if (li[1][j] < 0) continue;
+      const float wxy = wx[i] * wy[j];
+      typename A::T* row_acc = acc + (li[0][i] * T + li[1][j]) * T;
+#pragma unroll
+      for (int k = 0; k < W; k++) {
+        if (li[2][k] < 0) continue;
+        A::add(row_acc + li[2][k], wxy * wz[k]);
+      }
+    }
+  }
+}
+
+template <int T, int ASSIGN, bool EXACT>
+__global__ void __launch_bounds__(kDepThreads, 3) k_deposit(DepositArgs a) {
   constexpr int W = Width<ASSIGN>::W;
   using A = DepAcc<EXACT>;
   extern __shared__ __align__(16) unsigned char dep_smem[];
   typename A::T* acc = reinterpret_cast<typename A::T*>(dep_smem);
+  int32_t* s_list = reinterpret_cast<int32_t*>(dep_smem + sizeof(typename A::T) * T * T * T);
+  __shared__ int s_n;
+  // run start particle, run length, candidate offset of each run
+  __shared__ int32_t s_rb[kDepRuns], s_len[kDepRuns], s_rp[kDepRuns + 1];
+  static_assert(kDepRuns == 64, "two runs per lane of one warp");
+  const int lane = threadIdx.x & 31;
   const int N = a.N, C = a.C;
   int tb = blockIdx.x;
   const int tz = tb % a.ntile;
@@ -133,6 +184,7 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
   int ext[3];
   for (int d = 0; d < 3; d++) ext[d] = min(T, N - o[d]);
   for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) acc[i] = 0;
+  if (threadIdx.x == 0) s_n = 0;
   // chain cells whose particles can reach the tile: XN in [o-2, o+T+1)
   int clo[3], cnt[3];
   for (int d = 0; d < 3; d++) {
@@ -143,76 +195,109 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a) {
     if (cnt[d] == C) clo[d] = 0;
   }
   __syncthreads();
-  for (int iz = 0; iz < cnt[2]; iz++) {
-    const int cz = wrapi(clo[2] + iz, C);
-    for (int iy = 0; iy < cnt[1]; iy++) {
-      const int cy = wrapi(clo[1] + iy, C);
-      const int64_t row = ((int64_t)cz * C + cy) * C;
-      // x cells clo..clo+cnt-1 (mod C): one or two contiguous runs
-      const int x0 = wrapi(clo[0], C);
-      const int xend = x0 + cnt[0];
-      for (int part = 0; part < 2; part++) {
-        int ca, cb;
-        if (part == 0) {
-          ca = x0;
-          cb = min(xend, C);
-        } else {
-          if (xend <= C) break;
-          ca = 0;
-          cb = xend - C;
-        }
-        const int32_t pb = __ldg(a.begin + row + ca), pe = __ldg(a.begin + row + cb);
-        for (int32_t p = pb + threadIdx.x; p < pe; p += blockDim.x) {
-          const int4 q = __ldg(a.pos4 + p);
-          // first stencil point per dim relative to the tile, wrapped into
-          // [-N/2, N/2): the particle touches the tile only if every dim's
-          // W points meet [0, ext)
-          const int s0 = (int)(((uint64_t)(uint32_t)q.x * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
-          const int s1 = (int)(((uint64_t)(uint32_t)q.y * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
-          const int s2 = (int)(((uint64_t)(uint32_t)q.z * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
-          if (!touches<W>(s0 - o[0], N, ext[0]) || !touches<W>(s1 - o[1], N, ext[1]) ||
-              !touches<W>(s2 - o[2], N, ext[2]))
-            continue;
-          float wx[4], wy[4], wz[4];
-          int r[3];
-          r[0] = stencil<ASSIGN>((uint32_t)q.x, N, wx) - o[0];
-          r[1] = stencil<ASSIGN>((uint32_t)q.y, N, wy) - o[1];
-          r[2] = stencil<ASSIGN>((uint32_t)q.z, N, wz) - o[2];
-          int li[3][4];
-          bool any = true;
-          for (int d = 0; d < 3; d++) {
-            bool hit = false;
+  // Deposit the listed particles, all threads sharing the list; called by
+  // every thread with the list complete (after a barrier).  The list holds
+  // particles in their sorted (spatially compact) order, and the FP32 shared
+  // atomics are compare-and-swap loops that retry while lanes of a warp hit
+  // the same point: so the 32 lanes of a warp take entries S = ceil(n / 32)
+  // apart (slot u = lane + 32 c takes entry lane S + c, a bijection onto
+  // [0, n) over u < 32 S).
+  auto flush = [&]() {
+    const int n = s_n;
+    const int S = (n + 31) >> 5;
+    for (int u = threadIdx.x; u < 32 * S; u += kDepThreads) {
+      const int e = (u & 31) * S + (u >> 5);
+      if (e < n) deposit_particle<T, ASSIGN, EXACT>(acc, __ldg(a.pos4 + s_list[e]), N, o, ext);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+  };
+  // x cells clo..clo+cnt-1 (mod C) of a (z, y) row: one or two contiguous runs
+  const int x0 = wrapi(clo[0], C);
+  const int xend = x0 + cnt[0];
+  const int nparts = xend > C ? 2 : 1;
+  const int nrows = cnt[2] * cnt[1];
+  constexpr int kRowsPerBatch = kDepRuns / 2;
+  for (int row0 = 0; row0 < nrows; row0 += kRowsPerBatch) {
+    // run table of rows [row0, row0 + kRowsPerBatch): run t = row t / 2,
+    // part t % 2 (empty where the row or the part does not exist), lengths
+    // turned into candidate offsets by a warp scan
+    if (threadIdx.x < kDepRuns) {
+      const int t = threadIdx.x, rw = row0 + (t >> 1), part = t & 1;
+      int32_t pb = 0, len = 0;
+      if (rw < nrows && part < nparts) {
+        const int cz = wrapi(clo[2] + rw / cnt[1], C), cy = wrapi(clo[1] + rw % cnt[1], C);
+        const int64_t row = ((int64_t)cz * C + cy) * C;
+        const int ca = part == 0 ? x0 : 0, cb = part == 0 ? min(xend, C) : xend - C;
+        pb = __ldg(a.begin + row + ca);
+        len = __ldg(a.begin + row + cb) - pb;
+      }
+      s_rb[t] = pb;
+      s_len[t] = len;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int l = threadIdx.x;
+      const int32_t a0 = s_len[2 * l], a1 = s_len[2 * l + 1];
+      int32_t incl = a0 + a1;
 #pragma unroll
-            for (int k = 0; k < W; k++) {
-              int l = r[d] + k;
-              if (l < 0) l += N;
-              else if (l >= N) l -= N;
-              li[d][k] = l < ext[d] ? l : -1;
-              hit |= l < ext[d];
-            }
-            any &= hit;
-          }
-          if (!any) continue;
+      for (int off = 1; off < 32; off <<= 1) {
+        const int32_t v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (l >= off) incl += v;
+      }
+      s_rp[2 * l] = incl - a0 - a1;
+      s_rp[2 * l + 1] = incl - a1;
+      if (l == 31) s_rp[kDepRuns] = incl;
+    }
+    __syncthreads();
+    const int total = s_rp[kDepRuns];
+    int r = 0;  // this thread's run: candidates only increase
+    for (int base = 0; base < total; base += kDepThreads * kDepBatch) {
+      int32_t idx[kDepBatch];
+      int4 q[kDepBatch];
 #pragma unroll
-          for (int i = 0; i < W; i++) {
-            if (li[0][i] < 0) continue;
-#pragma unroll
-            for (int j = 0; j < W; j++) {
-              if (li[1][j] < 0) continue;
-              const float wxy = wx[i] * wy[j];
-              typename A::T* row_acc = acc + (li[0][i] * T + li[1][j]) * T;
-#pragma unroll
-              for (int k = 0; k < W; k++) {
-                if (li[2][k] < 0) continue;
-                A::add(row_acc + li[2][k], wxy * wz[k]);
-              }
-            }
-          }
+      for (int b = 0; b < kDepBatch; b++) {
+        const int cnd = base + b * kDepThreads + (int)threadIdx.x;
+        idx[b] = -1;
+        if (cnd < total) {
+          while (s_rp[r + 1] <= cnd) r++;
+          idx[b] = s_rb[r] + (cnd - s_rp[r]);
+          q[b] = __ldg(a.pos4 + idx[b]);
         }
       }
+      int end = 0;
+#pragma unroll
+      for (int b = 0; b < kDepBatch; b++) {
+        bool reach = false;
+        if (idx[b] >= 0) {
+          // first stencil point per dim relative to the tile, wrapped into
+          // [-N/2, N/2): the particle reaches the tile only if every dim's
+          // W points meet [0, ext)
+          const int s0 = (int)(((uint64_t)(uint32_t)q[b].x * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
+          const int s1 = (int)(((uint64_t)(uint32_t)q[b].y * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
+          const int s2 = (int)(((uint64_t)(uint32_t)q[b].z * (uint64_t)N) >> 32) + kStencilOff<ASSIGN>;
+          reach = touches<W>(s0 - o[0], N, ext[0]) && touches<W>(s1 - o[1], N, ext[1]) &&
+                  touches<W>(s2 - o[2], N, ext[2]);
+        }
+        // append to the list: one counter update per warp
+        const unsigned m = __ballot_sync(0xffffffffu, reach);
+        if (m) {
+          int b0 = 0;
+          if (lane == 0) b0 = atomicAdd(&s_n, __popc(m));
+          b0 = __shfl_sync(0xffffffffu, b0, 0);
+          if (reach) s_list[b0 + __popc(m & ((1u << lane) - 1u))] = idx[b];
+          end = max(end, b0 + __popc(m));
+        }
+      }
+      // the list holds at most kDepList - kDepThreads kDepBatch entries
+      // before a batch: deposit it once the next batch could overflow it
+      // (the warp that appended last knows the list's length)
+      if (__syncthreads_or(end > kDepList - kDepThreads * kDepBatch)) flush();
     }
+    __syncthreads();  // the run table is rebuilt for the next rows
   }
-  __syncthreads();
+  if (s_n > 0) flush();
   for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) {
     const int lz = i % T, ly = (i / T) % T, lx = i / (T * T);
     if (lx < ext[0] && ly < ext[1] && lz < ext[2])
@@ -294,7 +379,7 @@ template <int T, bool EXACT>
 int launch_deposit_T(tpm_ctx* c, DepositArgs a) {
   a.ntile = ceil_div(c->N, T);
   const int blocks = a.ntile * a.ntile * a.ntile;
-  const size_t smem = sizeof(typename DepAcc<EXACT>::T) * T * T * T;
+  const size_t smem = sizeof(typename DepAcc<EXACT>::T) * T * T * T + sizeof(int32_t) * kDepList;
   a.scale = 4.0 * M_PI * c->N * (EXACT ? std::ldexp(1.0, -kDepositFracBits) : 1.0);
   switch (c->opt.assign) {
     case TPM_ASSIGN_CIC:
