@@ -18,15 +18,23 @@
 //       two rows of phi
 //
 // The spectrum lives in a [N][N][Sz] complex array, Sz = N/2+1 rounded up to
-// the lines per block (4) so that a block's kz columns start on a 32-byte
-// boundary (the padding columns are zero and never reach phi).  Each block
-// holds 4 lines of length N in shared memory and transforms them with a
-// self-sorting (Stockham)
-// radix-16/8/4/3/5/2 FFT, each stage from one shared buffer into the other.  Twiddles
-// exp(-2 pi i m / N) are computed in FP64 on the host and staged in shared
-// memory.  Forward transforms use exp(-i...), inverse exp(+i...), both
-// unnormalised (cuFFT's convention); 1/N^3 is folded into the Green's
-// function.
+// 8 so that a block's kz columns start on a 64-byte boundary (the padding
+// columns are zero and never reach phi).  Two engines run the passes:
+//
+//  * line engine (the meshes with a compiled plan, TPM_LINE_SIZES): one line
+//    per TL lanes of a warp, E = N / TL values per lane in registers, a
+//    compile-time Stockham plan of radices 16/12/10/8/6/5/4/3/2 that divide E
+//    (three stages for most sizes: 12.8.8 at 768, 12.8.4 at 384), the line's
+//    row of shared memory between stages with warp-level synchronisation only,
+//    and per-stage twiddle tables; the x pass runs its inverse with the
+//    reversed plan straight from the forward transform's registers;
+//  * block engine (every other supported N): each block holds 4 lines in
+//    shared memory and transforms them with a radix-16/8/4/3/5/2 Stockham FFT
+//    over two shared buffers.
+//
+// Twiddles are computed in FP64 on the host.  Forward transforms use
+// exp(-i...), inverse exp(+i...), both unnormalised (cuFFT's convention);
+// 1/N^3 is folded into the Green's function.
 #include "tpm_internal.cuh"
 
 #include <cmath>
@@ -546,8 +554,6 @@ struct LineFft {
   using L = LineCfg<N>;
   static constexpr LinePlan P = REV ? reverse_plan(L::P) : L::P;
   static constexpr int TL = L::TL, E = L::E;
-  // butterfly stride of the last stage: output r of butterfly j is j + r NL
-  static constexpr int NL = N / P.rad[P.ns - 1];
 
   // Stage ST: v holds its inputs, v[b R + r] = x[j + r N / R] for the lane's
   // butterflies j = lane + TL b; twiddles exp(S 2 pi i (j mod Ns) r / (Ns R))
@@ -623,7 +629,8 @@ struct LineFft {
   }
 
   // The transform from inputs already in v (as load leaves them); out(n, value)
-  // takes output n, and v keeps the outputs, v[b R + r] = X[lane + TL b + r NL].
+  // takes output n, and v keeps the outputs, v[b R + r] = X[lane + TL b + r N / R]
+  // with R the last stage's radix.
   template <class Out>
   __device__ __forceinline__ static void from_regs(float2* __restrict__ line, float2 (&v)[E],
                                                    const float2* __restrict__ tw, int lane, Out out) {
@@ -785,13 +792,13 @@ __global__ void __launch_bounds__(LineCfg<N>::kThreads, LineCfg<N>::kMinBlocks)
   Fwd::load(v, lane, [&](int n) { return line[n]; });
   __syncwarp();
   Fwd::from_regs(line, v, s_tw, lane, [](int, float2) {});
-  // v[b R + r] = X[lane + TL b + r NL]: the Green's function in registers
+  // v[b RL + r] = X[lane + TL b + r N / RL]: the Green's function in registers
   constexpr int RL = Fwd::P.rad[Fwd::P.ns - 1];
 #pragma unroll
   for (int b = 0; b < L::E / RL; b++)
 #pragma unroll
     for (int r = 0; r < RL; r++) {
-      const int n = lane + L::TL * b + r * Fwd::NL;
+      const int n = lane + L::TL * b + r * (N / RL);
       const float k2 = __ldg(k2tab + n) + k2yz;
       const float g = k2 > 0.0f ? -(__ldg(gt + n) * gyz) * __frcp_rn(k2) * norm : 0.0f;
       v[b * RL + r] = make_float2(v[b * RL + r].x * g, v[b * RL + r].y * g);
