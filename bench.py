@@ -79,6 +79,39 @@ def replica_rate(n_per_rank, world, steps, ms):
     return n_per_rank * world * steps / (ms * 1e-3)
 
 
+def hbm_peak_gbs():
+    """Measured copy bandwidth of this pool's B200s (MEASURED_PEAKS.json), or
+    the pool's earlier measurement when the file is absent."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, copy)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback (6.65 TB/s, an earlier measurement on this pool)"
+
+
+def stage_hbm(grid, n, stages):
+    """HBM fractions of the long-range stages: algorithmic bytes per step
+    (each array read or written once: packed positions 16 B per particle,
+    the real mesh 4 N^3 B, the half spectrum 8 N^2 (N/2+1) B, results 16 B
+    and rung 1 B per particle) over the event-timed stage, against the
+    measured copy bandwidth."""
+    mesh = 4 * grid ** 3
+    spec = 8 * grid * grid * (grid // 2 + 1)
+    algo = {"deposit_ms": 16 * n + mesh,                      # positions in, density out
+            "fft_forward_ms": (mesh + spec) + 2 * spec,       # z (real -> half spectrum), y
+            "green_ms": 2 * spec,                             # x forward + Green + x inverse
+            "fft_inverse_ms": 2 * spec + (spec + mesh),       # y, z (half spectrum -> real)
+            "interp_ms": mesh + 16 * n + n + 16 * n}          # phi, positions, rung in; g, pot out
+    peak, source = hbm_peak_gbs()
+    out = {"peak_gbs": peak, "peak_source": source}
+    for k, b in algo.items():
+        ms = stages.get(k)
+        if ms:
+            gbs = b / (ms * 1e-3) / 1e9
+            out[k[:-3]] = {"bytes": int(b), "gbs": round(gbs, 1), "frac": round(gbs / peak, 3)}
+    return out
+
+
 def make_particles(cfg, seed):
     from tigerpm_b200 import workloads as W
     if cfg["kind"] == "uniform":
@@ -259,6 +292,7 @@ def gpu_arm(args, cfg, name, rank, world, dist):
                 "serial": {"value": total / (ms_serial * 1e-3), "ms_per_step": ms_serial / args.steps,
                            "api": "tpm_set_particles + tpm_pme_step + tpm_get_particles"}},
         "stages_ms": {k: round(v, 4) for k, v in stages.items() if v > 0},
+        "stages_hbm": stage_hbm(cfg["grid"], n, stages),
         "gpu_launches": int(launches), "clocks": clk.summary(),
     }
     # roofline of the dominant kernel (PP: FP32-bound)
@@ -376,12 +410,15 @@ def batch_arm(args, rank, world, dist, n_boxes=64, lo=32, hi=128):
             "speedup_vs_sequential": round(ms_seq / ms, 3), "accuracy": acc}
 
 
-def serve_arm(args, rank, world, dist, pool=256, lo=32, hi=192, rate=200.0, seconds=12.0, slots=8):
+def serve_arm(args, rank, world, dist, pool=256, lo=32, hi=192, rate=200.0, seconds=12.0, slots=32):
     """Config 5: a resident pool of `pool` Zel'dovich boxes (sides
     log-uniform in [lo, hi], generated on the device, each on its own mesh),
     kick + drift requests arriving as a Poisson process at `rate` per second
     for `seconds`, admitted by the HBM budget into up to `slots` concurrent
-    steps.  Latency = submission to completion (host clock)."""
+    steps.  Latency = submission to completion (host clock).  The offered
+    load (~2.7e8 particle-kicks/s) is close to what the slots sustain: with
+    8 slots a 12 s replay could fall behind it (p50 1 s), with 16 or 32 it
+    keeps up (p50 13 ms)."""
     from tigerpm_b200 import workloads as W
     from tigerpm_b200.api import Server, TigerPM, ic_zeldovich
     g = W.rng(args.seed + 90 + rank)
@@ -637,7 +674,8 @@ def main():
                 "data": "synthetic (seeded Philox; Zel'dovich / uniform as configured)",
                 "config": dict(workload_desc(args.config, cfg, opts), parallelism=f"replicas x{world}"),
                 "e2e": res["e2e"], "roofline": res["roofline"], "gpu_launches": res["gpu_launches"],
-                "clocks": res["clocks"], "stages_ms": res["stages_ms"], "accuracy": res.get("accuracy")}
+                "clocks": res["clocks"], "stages_ms": res["stages_ms"], "stages_hbm": res["stages_hbm"],
+                "accuracy": res.get("accuracy")}
         if batch is not None:
             batch["vs_plain_single_box"] = round(batch["value"] / res["value"], 4)
             line["batch"] = batch
