@@ -583,6 +583,14 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
           bzl = fminf(bzl, __shfl_xor_sync(0xffffffffu, bzl, o));
           bzh = fmaxf(bzh, __shfl_xor_sync(0xffffffffu, bzh, o));
         }
+        // box as centre and half-extent: the distance along an axis is then
+        // |s - c| - h (3 instructions instead of 4).  The half-extent is
+        // widened by 1e-5 of the unit (2 r_s; offsets here are a few units,
+        // whose float spacing is < 1e-6) to cover the rounding of c, h and
+        // s - c, so the cull never drops a source the exact pair test keeps.
+        const float cbx = 0.5f * (bxl + bxh), hbx = fmaf(0.5f, bxh - bxl, 1e-5f);
+        const float cby = 0.5f * (byl + byh), hby = fmaf(0.5f, byh - byl, 1e-5f);
+        const float cbz = 0.5f * (bzl + bzh), hbz = fmaf(0.5f, bzh - bzl, 1e-5f);
         float px = 0.f, py = 0.f, pz = 0.f, pp = 0.f;
         int cnt = 0;
         for (int j0 = 0; j0 < len; j0 += 32) {
@@ -592,9 +600,9 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
           if (keep) {
             s = src[j];
             if (cull) {
-              const float ex = fmaxf(fmaxf(bxl - s.x, s.x - bxh), 0.f);
-              const float ey = fmaxf(fmaxf(byl - s.y, s.y - byh), 0.f);
-              const float ez = fmaxf(fmaxf(bzl - s.z, s.z - bzh), 0.f);
+              const float ex = fmaxf(fabsf(s.x - cbx) - hbx, 0.f);
+              const float ey = fmaxf(fabsf(s.y - cby) - hby, 0.f);
+              const float ez = fmaxf(fabsf(s.z - cbz) - hbz, 0.f);
               keep = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.rcut2;
             }
           }
