@@ -10,14 +10,15 @@
 // Device design:
 //  * deposit: "owner computes" mesh tiles.  One block owns a T^3 tile of the
 //    grid, reads the particles of the chain cells whose assignment stencils
-//    can reach it (particles are already in chain-cell order), and
-//    accumulates the weights in shared memory; each grid point is written
-//    once, with no global atomics and no zeroing pass.  Accumulation is FP32
-//    shared atomics by default, or (deterministic_deposit) exact 40-bit
-//    fixed point in int64, whose integer sums are bit-for-bit reproducible
-//    whatever the thread order.
-//  * FFT: cuFFT r2c / c2r (the library the project allows here), timed as
-//    its own stages.
+//    can reach it (particles are already in chain-cell order), compacts the
+//    ones that reach it into a shared list and accumulates their weights in
+//    shared memory; each grid point is written once, with no global atomics
+//    and no zeroing pass.  Accumulation is FP32 shared atomics by default,
+//    or (deterministic_deposit) exact 40-bit fixed point in int64, whose
+//    integer sums are bit-for-bit reproducible whatever the thread order.
+//  * FFT: the library's own five-pass transforms (fft3d.cu) for meshes of
+//    the form 2^a 3^b 5^c that are multiples of 16, else (or with fft =
+//    cufft) cuFFT r2c / c2r around k_green; each timed as its own stages.
 //  * Green's function: exp(-k^2 rs^2) * sinc(k/2)^-p factorises per axis, so
 //    a per-index table (built in FP64 on the host) and k^2 = kx^2+ky^2+kz^2
 //    give G on the fly: one read + one write of the complex grid.
