@@ -553,12 +553,12 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
     __syncthreads();
     const int nact = runp[kMaxRuns + 1];
     const int ngroups = (nact + kGroup - 1) / kGroup;
+    int r = 0;  // this thread's neighbourhood run: its staged indices only increase
     for (int c0 = 0; c0 < total; c0 += stage) {
       const int len = min(stage, total - c0);
       __syncthreads();
       for (int j = tid; j < len; j += T) {
         const int e = c0 + j;
-        int r = 0;
         while (runp[r + 1] <= e) r++;
         const int4 u = __ldg(a.pos4 + runb[r] + (e - runp[r]));
         src[j] = make_float4(offset_scaled((uint32_t)u.x, ox, sc), offset_scaled((uint32_t)u.y, oy, sc),
