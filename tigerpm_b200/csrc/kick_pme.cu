@@ -780,30 +780,6 @@ __global__ void __launch_bounds__(kKickThreads, TPM_KICK_MINB)
   }
 }
 
-// Long-range interpolation of every item's sinks (one block per item,
-// direct reads).
-__global__ void __launch_bounds__(64) k_interp_batch(const KickArgs* __restrict__ boxes, const int4* __restrict__ items,
-                                                      const int* __restrict__ nitems, int min_rung, int npass) {
-  if ((int)blockIdx.x >= *nitems) return;
-  const int4 w = __ldg(items + blockIdx.x);
-  if (w.x < 0) return;  // empty slot
-  const KickArgs& a = boxes[w.x];
-  const int32_t pb = __ldg(a.begin + w.y), pe = __ldg(a.begin + w.y + 1);
-  int np = 8;
-  while (np < npass && np < pe - pb) np <<= 1;
-  const int32_t lo = pb + w.z * np;
-  const int32_t hi = (int32_t)min((int64_t)pe, (int64_t)pb + (int64_t)w.w * np);
-  for (int32_t i = lo + (int32_t)threadIdx.x; i < hi; i += blockDim.x) {
-    if (a.rung[i] < min_rung) continue;
-    float lx, ly, lz, lp;
-    interp_long(a, __ldg(a.pos4 + i), lx, ly, lz, lp);
-    a.gx[i] = lx;
-    a.gy[i] = ly;
-    a.gz[i] = lz;
-    a.pot[i] = lp;
-  }
-}
-
 // Work items: every non-empty (box, cell) of the kick boxes, bucketed by the
 // binary order of magnitude of its cost and laid out heaviest bucket first.
 // A cell with more sinks than one pass is split into one item per pass (a
@@ -924,6 +900,28 @@ __global__ void k_item_scatter(const BoxCells* __restrict__ bc, int nbox, int to
   items[nsplit + g] = make_int4(-1, 0, 0, 0);
   const int at = start[cl] + atomicAdd(fill + cl, k);
   for (int p = 0; p < k; p++) items[at + p] = make_int4(b, key, p, p + 1);
+}
+
+// Long-range interpolation of the batch: one block per global cell slot,
+// every box's cells in natural order, so that neighbouring cells' stencil
+// reads share the L1 and L2 as in the single-box k_interp_direct (in the
+// queue's cost order, items of different boxes interleave).
+__global__ void __launch_bounds__(64, TPM_INTERP_MINB)
+    k_interp_slots(const KickArgs* __restrict__ boxes, const BoxCells* __restrict__ bc, int nbox, int min_rung) {
+  const int g = blockIdx.x;
+  const int b = find_box(bc, nbox, g);
+  const KickArgs a = boxes[b];  // the fields used, in registers
+  const int key = g - __ldg(&bc[b].base);
+  const int32_t pb = __ldg(a.begin + key), pe = __ldg(a.begin + key + 1);
+  for (int32_t i = pb + (int32_t)threadIdx.x; i < pe; i += blockDim.x) {
+    if (a.rung[i] < min_rung) continue;
+    float lx, ly, lz, lp;
+    interp_long(a, __ldg(a.pos4 + i), lx, ly, lz, lp);
+    a.gx[i] = lx;
+    a.gy[i] = ly;
+    a.gz[i] = lz;
+    a.pot[i] = lp;
+  }
 }
 
 // The batch's ordinary cells: one block per global cell slot (every box's
@@ -1128,9 +1126,10 @@ int kick_batch_queue(const BatchQueue& q, int npass, cudaStream_t s) {
 }
 
 int kick_batch_interp(const BatchQueue& q, int min_rung, int npass, cudaStream_t s) {
+  (void)npass;
   if (q.total_cells <= 0) return TPM_OK;
-  k_interp_batch<<<(unsigned)q.max_items, 64, 0, s>>>(static_cast<const KickArgs*>(q.d_args), q.d_items,
-                                                       q.d_nitems, min_rung, npass);
+  k_interp_slots<<<(unsigned)q.total_cells, 64, 0, s>>>(static_cast<const KickArgs*>(q.d_args),
+                                                         static_cast<const BoxCells*>(q.d_cells), q.nbox, min_rung);
   TPM_CUDA_TRY(cudaGetLastError());
   return TPM_OK;
 }
