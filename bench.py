@@ -299,12 +299,21 @@ def gpu_arm(args, cfg, name, rank, world, dist):
     cand, inside = ctx.count_pairs(0)
     flops = FLOPS_PER_PAIR * inside + FLOPS_PER_CULLED * (cand - inside)
     kick_ms = stages["kick_ms"]
-    peak = fp32_peak_probe()
+    # the FP32 peak: the FMA-chain probe repeated for ~1 s with the SM clock
+    # sampled meanwhile (the median probe value, and the clock it ran at)
+    probes = []
+    with ClockSampler(dev.index) as pclk:
+        t_probe = time.perf_counter()
+        while len(probes) < 3 or time.perf_counter() - t_probe < 1.0:
+            probes.append(fp32_peak_probe())
+    peak = statistics.median(probes)
     achieved = flops / (kick_ms * 1e-3) / 1e12
     out["roofline"] = {"bound": "fp32", "kernel": "k_kick_pme", "achieved": round(achieved, 3),
                        "peak": round(peak, 2), "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
                        "traffic": read_traffic(name),
-                       "peak_source": "measured FP32 FMA probe on this GPU (tpm_fp32_peak_probe)",
+                       "peak_source": "measured FP32 FMA probe on this GPU (tpm_fp32_peak_probe, median of "
+                                      f"{len(probes)})",
+                       "peak_clocks": pclk.summary(),
                        "pairs_in_cutoff": inside, "pairs_candidate": cand,
                        "flops_per_launch": flops, "kick_ms": round(kick_ms, 4)}
     # accuracy of this kick vs the FP64 Ewald sum
