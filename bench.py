@@ -314,6 +314,8 @@ def gpu_arm(args, cfg, name, rank, world, dist):
                        "peak_source": "measured FP32 FMA probe on this GPU (tpm_fp32_peak_probe, median of "
                                       f"{len(probes)})",
                        "peak_clocks": pclk.summary(),
+                       # the same kernel credited with the in-cutoff pairs' flops only
+                       "frac_in_cutoff_only": round(FLOPS_PER_PAIR * inside / (kick_ms * 1e-3) / 1e12 / peak, 4),
                        "pairs_in_cutoff": inside, "pairs_candidate": cand,
                        "flops_per_launch": flops, "kick_ms": round(kick_ms, 4)}
     # accuracy of this kick vs the FP64 Ewald sum
