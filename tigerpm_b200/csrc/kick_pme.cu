@@ -471,7 +471,10 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int t8 = lane & 7, ph = lane >> 3;
   const float Cf = (float)C;
-  const bool cull = !WRAP && a.rcut2 < INFINITY;  // culling works on unwrapped offsets
+  // culling works on unwrapped offsets; without it every source is kept
+  const float keep2 = !WRAP && a.rcut2 < INFINITY ? a.rcut2 : INFINITY;
+  unsigned lt;  // lanes below this one
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
   const float sc = a.lscale;
   const PairK pk{a.rcut2, a.h2, a.inv2rs};
   if (tid == 0) {
@@ -593,24 +596,22 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
         const float cbz = 0.5f * (bzl + bzh), hbz = fmaf(0.5f, bzh - bzl, 1e-5f);
         float px = 0.f, py = 0.f, pz = 0.f, pp = 0.f;
         int cnt = 0;
+        // Every lane loads a staged source (the last one again past the end)
+        // and tests it; kept sources are appended to the warp's buffer.  The
+        // buffer is read only after a __syncwarp (flush or tail), so appends
+        // need no barrier of their own.
         for (int j0 = 0; j0 < len; j0 += 32) {
           const int j = j0 + lane;
-          bool keep = j < len;
-          float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (keep) {
-            s = src[j];
-            if (cull) {
-              const float ex = fmaxf(fabsf(s.x - cbx) - hbx, 0.f);
-              const float ey = fmaxf(fabsf(s.y - cby) - hby, 0.f);
-              const float ez = fmaxf(fabsf(s.z - cbz) - hbz, 0.f);
-              keep = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.rcut2;
-            }
-          }
+          const float4 s = src[min(j, len - 1)];
+          const float ex = fmaxf(fabsf(s.x - cbx) - hbx, 0.f);
+          const float ey = fmaxf(fabsf(s.y - cby) - hby, 0.f);
+          const float ez = fmaxf(fabsf(s.z - cbz) - hbz, 0.f);
+          const bool keep = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < keep2 && j < len;
           const unsigned b = __ballot_sync(0xffffffffu, keep);
-          if (keep) buf[cnt + __popc(b & ((1u << lane) - 1u))] = s;
+          if (keep) buf[cnt + __popc(b & lt)] = s;
           cnt += __popc(b);
-          __syncwarp();
           if (cnt >= 32) {
+            __syncwarp();
 #pragma unroll
             for (int k = 0; k < 32; k += 4) {
               const float4 u = buf[k + ph];
@@ -622,6 +623,7 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
             __syncwarp();
           }
         }
+        __syncwarp();
         for (int k = 0; k < cnt; k += 4) {
           if (k + ph < cnt && mysink) {
             const float4 u = buf[k + ph];
