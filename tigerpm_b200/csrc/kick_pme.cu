@@ -367,7 +367,10 @@ struct PairK {
 // is needed only when chain_dim = 3, where the 27 cells span the whole box
 // and an offset from the cell centre can exceed half the box.  Sums are in
 // the scaled units: force x 1/(2 r_s)^2, potential x 1/(2 r_s).
-template <bool WRAP>
+// CONVERGED: every lane of the warp calls it together; the softened branch
+// is then taken only when some lane of the warp needs it (a warp vote), and
+// inside it each lane selects its own result.
+template <bool WRAP, bool CONVERGED = false>
 __device__ __forceinline__ void pair(const PairK& k, float dx, float dy, float dz, float& gx, float& gy, float& gz,
                                      float& ph) {
   if (WRAP) {
@@ -393,11 +396,14 @@ __device__ __forceinline__ void pair(const PairK& k, float dx, float dy, float d
   // (erfc + (2/sqrt(pi)) r e) / r^3 = (erfc / r + (2/sqrt(pi)) e) / r^2
   float q = poly * e * rinv;
   float rinv3 = fmaf(1.1283791670955126f, e, q) * (rinv * rinv);
-  if (r2 <= k.h2) {  // softened Newtonian kernel inside hsoft (rare)
+  const bool soft = r2 <= k.h2;  // softened Newtonian kernel inside hsoft (rare)
+  if (CONVERGED ? __any_sync(0xffffffffu, soft) : soft) {
     const float hinv = rsqrtf(k.h2);
     const float q2 = r2 * hinv * hinv;
-    rinv3 = fmaf(fmaf(15.0f / 8.0f, q2, -21.0f / 4.0f), q2, 35.0f / 8.0f) * (hinv * hinv * hinv);
-    q = fmaf(fmaf(fmaf(-5.0f / 16.0f, q2, 21.0f / 16.0f), q2, -35.0f / 16.0f), q2, 35.0f / 16.0f) * hinv;
+    const float s3 = fmaf(fmaf(15.0f / 8.0f, q2, -21.0f / 4.0f), q2, 35.0f / 8.0f) * (hinv * hinv * hinv);
+    const float s1 = fmaf(fmaf(fmaf(-5.0f / 16.0f, q2, 21.0f / 16.0f), q2, -35.0f / 16.0f), q2, 35.0f / 16.0f) * hinv;
+    rinv3 = soft ? s3 : rinv3;
+    q = soft ? s1 : q;
   }
   gx = fmaf(-dx, rinv3, gx);
   gy = fmaf(-dy, rinv3, gy);
@@ -614,8 +620,10 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
             __syncwarp();
 #pragma unroll
             for (int k = 0; k < 32; k += 4) {
+              // lanes without a sink (a partial group) hold a copy of the
+              // group's first sink; their sums are never committed
               const float4 u = buf[k + ph];
-              if (mysink) pair<WRAP>(pk, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
+              pair<WRAP, true>(pk, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
             }
             __syncwarp();
             if (lane < cnt - 32) buf[lane] = buf[32 + lane];
