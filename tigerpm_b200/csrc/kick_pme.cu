@@ -633,9 +633,16 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
         }
         __syncwarp();
         for (int k = 0; k < cnt; k += 4) {
-          if (k + ph < cnt && mysink) {
-            const float4 u = buf[k + ph];
-            pair<WRAP>(pk, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
+          if (WRAP) {
+            if (k + ph < cnt && mysink) {
+              const float4 u = buf[k + ph];
+              pair<WRAP>(pk, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
+            }
+          } else {
+            // past the count a lane takes a source 1e18 units away: beyond
+            // any cutoff, its terms are exactly 0 (no minimum-image fold here)
+            const float4 u = k + ph < cnt ? buf[k + ph] : make_float4(1e18f, 1e18f, 1e18f, 0.f);
+            pair<WRAP, true>(pk, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
           }
         }
         __syncwarp();
