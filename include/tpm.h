@@ -103,7 +103,10 @@ typedef struct tpm_options {
   int sort_mode;       /* TPM_SORT_*; default PARITY */
   int kahan;           /* 1: compensated per-target PP sums (default 1) */
   int deterministic_deposit; /* 1: exact int64 fixed-point deposit, bit-reproducible;
-                              * 0: FP32 shared-memory atomics (default, faster) */
+                              * 0 (default, faster): 26-bit fixed point in uint32,
+                              * bit-reproducible unless a mesh tile holds 16 or more
+                              * weight units at one point, which is then deposited
+                              * again with FP32 shared-memory atomics */
   int fft;             /* TPM_FFT_*: 3-D transforms of gravity_long_compute */
   uint64_t seed;       /* synthetic-input seed carried for drivers */
   int fft_group;       /* x-planes per launch of the library FFT's z / y passes

@@ -13,9 +13,11 @@
 //    can reach it (particles are already in chain-cell order), compacts the
 //    ones that reach it into a shared list and accumulates their weights in
 //    shared memory; each grid point is written once, with no global atomics
-//    and no zeroing pass.  Accumulation is FP32 shared atomics by default,
-//    or (deterministic_deposit) exact 40-bit fixed point in int64, whose
-//    integer sums are bit-for-bit reproducible whatever the thread order.
+//    and no zeroing pass.  Accumulation is 26-bit fixed point with native
+//    32-bit shared integer adds by default (a tile that could overflow is
+//    deposited again with FP32 atomics), or (deterministic_deposit) exact
+//    40-bit fixed point in int64; integer sums are bit-for-bit reproducible
+//    whatever the thread order.
 //  * FFT: the library's own five-pass transforms (fft3d.cu) for meshes of
 //    the form 2^a 3^b 5^c that are multiples of 16, else (or with fft =
 //    cufft) cuFFT r2c / c2r around k_green; each timed as its own stages.
@@ -25,6 +27,7 @@
 #include "tpm_internal.cuh"
 
 #include <cmath>
+#include <type_traits>
 
 namespace tpm {
 namespace {
@@ -88,29 +91,51 @@ struct DepositArgs {
   int C;
   int N;
   int ntile;     // tiles per side
-  double scale;  // 4 pi N * 2^-40
+  double scale;  // 4 pi N (times the accumulator's fixed-point unit)
   float* __restrict__ rho;
 };
 
-// Accumulator of one tile point: exact 40-bit fixed point in int64 (order
-// independent, bit-reproducible) or FP32 shared atomics (faster, rounding
-// depends on the order in which threads reach a point).
-template <bool EXACT>
+// Accumulator of one tile point.
+//  kDepI32 (default): 26-bit fixed point in uint32 with the native shared
+//    integer add; sums are order independent (bit-reproducible).  Weights
+//    are at most 1, so an add never carries a point past 2^32 without some
+//    earlier value at or above 2^30: every add returns the old value, and a
+//    tile where any old value reached 2^30 (16 weight units at one point) is
+//    deposited again with kDepF32.
+//  kDepI64 (deterministic_deposit): exact 40-bit fixed point in int64.
+//  kDepF32: FP32 shared atomics (compare-and-swap loops; the rounding
+//    depends on the order in which threads reach a point).
+constexpr int kDepF32 = 0, kDepI64 = 1, kDepI32 = 2;
+constexpr int kDep32FracBits = 26;
+template <int M>
 struct DepAcc;
 template <>
-struct DepAcc<true> {
+struct DepAcc<kDepI64> {
   using T = unsigned long long;
-  static __device__ __forceinline__ void add(T* p, float w) {
+  static __device__ __forceinline__ void add(T* p, float w, unsigned&) {
     atomicAdd(p, (unsigned long long)__float2ll_rn(w * 1099511627776.0f));
   }
-  static __device__ __forceinline__ double value(T v, double scale) { return (double)(long long)v * scale; }
+  static __device__ __forceinline__ double value(T v, double scale) {
+    return (double)(long long)v * scale * 9.094947017729282e-13;  // 2^-40
+  }
 };
 template <>
-struct DepAcc<false> {
+struct DepAcc<kDepF32> {
   using T = float;
-  static __device__ __forceinline__ void add(T* p, float w) { atomicAdd(p, w); }
+  static __device__ __forceinline__ void add(T* p, float w, unsigned&) { atomicAdd(p, w); }
   static __device__ __forceinline__ double value(T v, double scale) { return (double)v * scale; }
 };
+template <>
+struct DepAcc<kDepI32> {
+  using T = unsigned;
+  static __device__ __forceinline__ void add(T* p, float w, unsigned& hi) {
+    hi |= atomicAdd(p, __float2uint_rn(w * 67108864.0f));  // 2^26
+  }
+  static __device__ __forceinline__ double value(T v, double scale) {
+    return (double)v * scale * 1.4901161193847656e-08;  // 2^-26
+  }
+};
+static_assert(kDep32FracBits == 26 && kDepositFracBits == 40, "fixed-point scales above");
 
 // The candidates of a tile (the particles of the chain cells that can reach
 // it: 9 to 16 rows of 3 to 4 x cells, up to twice 8x the tile's own) are one
@@ -124,12 +149,13 @@ constexpr int kDepBatch = 4;
 constexpr int kDepList = 2048;
 constexpr int kDepRuns = 64;
 
-// Weights of one particle added to the tile (stencil origin o, extent ext).
-template <int T, int ASSIGN, bool EXACT>
-__device__ __forceinline__ void deposit_particle(typename DepAcc<EXACT>::T* acc, int4 q, int N, const int (&o)[3],
-                                                 const int (&ext)[3]) {
+// Weights of one particle added to the tile (stencil origin o, extent ext);
+// hi collects the old values of kDepI32 adds.
+template <int T, int ASSIGN, int M>
+__device__ __forceinline__ void deposit_particle(typename DepAcc<M>::T* acc, int4 q, int N, const int (&o)[3],
+                                                 const int (&ext)[3], unsigned& hi) {
   constexpr int W = Width<ASSIGN>::W;
-  using A = DepAcc<EXACT>;
+  using A = DepAcc<M>;
   float wx[4], wy[4], wz[4];
   int r[3];
   r[0] = stencil<ASSIGN>((uint32_t)q.x, N, wx) - o[0];
@@ -157,19 +183,19 @@ __device__ __forceinline__ void deposit_particle(typename DepAcc<EXACT>::T* acc,
 #pragma unroll
       for (int k = 0; k < W; k++) {
         if (li[2][k] < 0) continue;
-        A::add(row_acc + li[2][k], wxy * wz[k]);
+        A::add(row_acc + li[2][k], wxy * wz[k], hi);
       }
     }
   }
 }
 
-template <int T, int ASSIGN, bool EXACT>
+template <int T, int ASSIGN, int M>
 __global__ void __launch_bounds__(kDepThreads, 3) k_deposit(DepositArgs a) {
   constexpr int W = Width<ASSIGN>::W;
-  using A = DepAcc<EXACT>;
   extern __shared__ __align__(16) unsigned char dep_smem[];
-  typename A::T* acc = reinterpret_cast<typename A::T*>(dep_smem);
-  int32_t* s_list = reinterpret_cast<int32_t*>(dep_smem + sizeof(typename A::T) * T * T * T);
+  // the list follows the tile (a kDepF32 redo of a kDepI32 tile uses the
+  // same 4-byte points)
+  int32_t* s_list = reinterpret_cast<int32_t*>(dep_smem + sizeof(typename DepAcc<M>::T) * T * T * T);
   __shared__ int s_n;
   // run start particle, run length, candidate offset of each run
   __shared__ int32_t s_rb[kDepRuns], s_len[kDepRuns], s_rp[kDepRuns + 1];
@@ -184,8 +210,6 @@ __global__ void __launch_bounds__(kDepThreads, 3) k_deposit(DepositArgs a) {
   const int o[3] = {tx * T, ty * T, tz * T};
   int ext[3];
   for (int d = 0; d < 3; d++) ext[d] = min(T, N - o[d]);
-  for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) acc[i] = 0;
-  if (threadIdx.x == 0) s_n = 0;
   // chain cells whose particles can reach the tile: XN in [o-2, o+T+1)
   int clo[3], cnt[3];
   for (int d = 0; d < 3; d++) {
@@ -195,6 +219,16 @@ __global__ void __launch_bounds__(kDepThreads, 3) k_deposit(DepositArgs a) {
     cnt[d] = min(hi - lo + 1, C);
     if (cnt[d] == C) clo[d] = 0;
   }
+  // The whole tile with accumulator mode MODE (its zeroing, the candidate
+  // scan and the deposits); returns, for kDepI32, whether a point may have
+  // overflowed.
+  auto deposit_tile = [&](auto mode) -> bool {
+  constexpr int MODE = decltype(mode)::value;
+  using A = DepAcc<MODE>;
+  typename A::T* acc = reinterpret_cast<typename A::T*>(dep_smem);
+  for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) acc[i] = 0;
+  if (threadIdx.x == 0) s_n = 0;
+  unsigned hi = 0;
   __syncthreads();
   // Deposit the listed particles, all threads sharing the list; called by
   // every thread with the list complete (after a barrier).  The list holds
@@ -208,7 +242,7 @@ __global__ void __launch_bounds__(kDepThreads, 3) k_deposit(DepositArgs a) {
     const int S = (n + 31) >> 5;
     for (int u = threadIdx.x; u < 32 * S; u += kDepThreads) {
       const int e = (u & 31) * S + (u >> 5);
-      if (e < n) deposit_particle<T, ASSIGN, EXACT>(acc, __ldg(a.pos4 + s_list[e]), N, o, ext);
+      if (e < n) deposit_particle<T, ASSIGN, MODE>(acc, __ldg(a.pos4 + s_list[e]), N, o, ext, hi);
     }
     __syncthreads();
     if (threadIdx.x == 0) s_n = 0;
@@ -299,10 +333,25 @@ __global__ void __launch_bounds__(kDepThreads, 3) k_deposit(DepositArgs a) {
     __syncthreads();  // the run table is rebuilt for the next rows
   }
   if (s_n > 0) flush();
-  for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) {
-    const int lz = i % T, ly = (i / T) % T, lx = i / (T * T);
-    if (lx < ext[0] && ly < ext[1] && lz < ext[2])
-      a.rho[((int64_t)(o[0] + lx) * N + (o[1] + ly)) * N + (o[2] + lz)] = (float)A::value(acc[i], a.scale);
+  if constexpr (MODE == kDepI32) return __syncthreads_or(hi >= (1u << 30)) != 0;
+  __syncthreads();
+  return false;
+  };
+  auto store_tile = [&](auto mode) {
+    constexpr int MODE = decltype(mode)::value;
+    using A = DepAcc<MODE>;
+    const typename A::T* acc = reinterpret_cast<const typename A::T*>(dep_smem);
+    for (int i = threadIdx.x; i < T * T * T; i += blockDim.x) {
+      const int lz = i % T, ly = (i / T) % T, lx = i / (T * T);
+      if (lx < ext[0] && ly < ext[1] && lz < ext[2])
+        a.rho[((int64_t)(o[0] + lx) * N + (o[1] + ly)) * N + (o[2] + lz)] = (float)A::value(acc[i], a.scale);
+    }
+  };
+  if (deposit_tile(std::integral_constant<int, M>{})) {
+    deposit_tile(std::integral_constant<int, kDepF32>{});
+    store_tile(std::integral_constant<int, kDepF32>{});
+  } else {
+    store_tile(std::integral_constant<int, M>{});
   }
 }
 
@@ -376,27 +425,27 @@ __global__ void k_force_at(const float* __restrict__ phi, int N, int64_t n, cons
   for (int d = 0; d < 3; d++) g_out[3 * p + d] = (float)(-g[d]);
 }
 
-template <int T, bool EXACT>
+template <int T, int M>
 int launch_deposit_T(tpm_ctx* c, DepositArgs a) {
   a.ntile = ceil_div(c->N, T);
   const int blocks = a.ntile * a.ntile * a.ntile;
-  const size_t smem = sizeof(typename DepAcc<EXACT>::T) * T * T * T + sizeof(int32_t) * kDepList;
-  a.scale = 4.0 * M_PI * c->N * (EXACT ? std::ldexp(1.0, -kDepositFracBits) : 1.0);
+  const size_t smem = sizeof(typename DepAcc<M>::T) * T * T * T + sizeof(int32_t) * kDepList;
+  a.scale = 4.0 * M_PI * c->N;
   switch (c->opt.assign) {
     case TPM_ASSIGN_CIC:
-      TPM_CUDA_TRY(cudaFuncSetAttribute(k_deposit<T, TPM_ASSIGN_CIC, EXACT>,
+      TPM_CUDA_TRY(cudaFuncSetAttribute(k_deposit<T, TPM_ASSIGN_CIC, M>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_deposit<T, TPM_ASSIGN_CIC, EXACT><<<blocks, 256, smem, c->stream>>>(a);
+      k_deposit<T, TPM_ASSIGN_CIC, M><<<blocks, 256, smem, c->stream>>>(a);
       break;
     case TPM_ASSIGN_TSC:
-      TPM_CUDA_TRY(cudaFuncSetAttribute(k_deposit<T, TPM_ASSIGN_TSC, EXACT>,
+      TPM_CUDA_TRY(cudaFuncSetAttribute(k_deposit<T, TPM_ASSIGN_TSC, M>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_deposit<T, TPM_ASSIGN_TSC, EXACT><<<blocks, 256, smem, c->stream>>>(a);
+      k_deposit<T, TPM_ASSIGN_TSC, M><<<blocks, 256, smem, c->stream>>>(a);
       break;
     default:
-      TPM_CUDA_TRY(cudaFuncSetAttribute(k_deposit<T, TPM_ASSIGN_CLOUD4, EXACT>,
+      TPM_CUDA_TRY(cudaFuncSetAttribute(k_deposit<T, TPM_ASSIGN_CLOUD4, M>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_deposit<T, TPM_ASSIGN_CLOUD4, EXACT><<<blocks, 256, smem, c->stream>>>(a);
+      k_deposit<T, TPM_ASSIGN_CLOUD4, M><<<blocks, 256, smem, c->stream>>>(a);
       break;
   }
   c->launches++;
@@ -456,10 +505,10 @@ int gravity_long(tpm_ctx* c, int type) {
   // tile edge: 24 points on large meshes (fewer redundant particle visits),
   // 16 / 8 on smaller ones; exact (int64) tiles of 24^3 would need 110 KB.
   if (c->opt.deterministic_deposit) {
-    rc = N >= 128 ? launch_deposit_T<16, true>(c, a) : launch_deposit_T<8, true>(c, a);
+    rc = N >= 128 ? launch_deposit_T<16, kDepI64>(c, a) : launch_deposit_T<8, kDepI64>(c, a);
   } else {
-    rc = N >= 192 ? launch_deposit_T<24, false>(c, a) : (N >= 64 ? launch_deposit_T<16, false>(c, a)
-                                                                  : launch_deposit_T<8, false>(c, a));
+    rc = N >= 192 ? launch_deposit_T<24, kDepI32>(c, a)
+                  : (N >= 64 ? launch_deposit_T<16, kDepI32>(c, a) : launch_deposit_T<8, kDepI32>(c, a));
   }
   if (rc) return rc;
   stage_end(c, kStDeposit);
