@@ -232,16 +232,18 @@ __global__ void __launch_bounds__(kDepThreads, 3) k_deposit(DepositArgs a) {
   __syncthreads();
   // Deposit the listed particles, all threads sharing the list; called by
   // every thread with the list complete (after a barrier).  The list holds
-  // particles in their sorted (spatially compact) order, and the FP32 shared
+  // particles in their sorted (spatially compact) order.  Consecutive
+  // entries go to consecutive lanes for the integer adds; the FP32 shared
   // atomics are compare-and-swap loops that retry while lanes of a warp hit
-  // the same point: so the 32 lanes of a warp take entries S = ceil(n / 32)
-  // apart (slot u = lane + 32 c takes entry lane S + c, a bijection onto
-  // [0, n) over u < 32 S).
+  // the same point, so there the 32 lanes of a warp take entries
+  // S = ceil(n / 32) apart (slot u = lane + 32 c takes entry lane S + c, a
+  // bijection onto [0, n) over u < 32 S).
   auto flush = [&]() {
     const int n = s_n;
-    const int S = (n + 31) >> 5;
-    for (int u = threadIdx.x; u < 32 * S; u += kDepThreads) {
-      const int e = (u & 31) * S + (u >> 5);
+    const int S = MODE == kDepF32 ? (n + 31) >> 5 : 0;
+    const int slots = MODE == kDepF32 ? 32 * S : n;
+    for (int u = threadIdx.x; u < slots; u += kDepThreads) {
+      const int e = MODE == kDepF32 ? (u & 31) * S + (u >> 5) : u;
       if (e < n) deposit_particle<T, ASSIGN, MODE>(acc, __ldg(a.pos4 + s_list[e]), N, o, ext, hi);
     }
     __syncthreads();
