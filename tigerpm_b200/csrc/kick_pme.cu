@@ -134,13 +134,14 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
   const int z0 = iz[0];
   const int a4 = z0 & ~3;
   if ((N & 3) == 0 && a4 + 12 <= N) {
-    // Each z-run of 6 points is read as three aligned float4 (12 points
-    // from a4 = z0 rounded down to 4); the z weights are shifted by
-    // s = z0 - a4 once per sink, zero outside the run.
+    // Each z-run of 6 points is read as two aligned float4 (8 points from
+    // a4 = z0 rounded down to 4) and, when the run starts at a4 + 3, one
+    // more float; the z weights are shifted by s = z0 - a4 once per sink,
+    // zero outside the run.
     const int s = z0 - a4;
-    float ws[12], dws[12];
+    float ws[9], dws[9];
 #pragma unroll
-    for (int m = 0; m < 12; m++) {
+    for (int m = 0; m < 9; m++) {
       float u = 0.f, du = 0.f;
 #pragma unroll
       for (int k = 0; k < kNInterp; k++) {
@@ -158,12 +159,13 @@ __device__ __forceinline__ void interp_long(const KickArgs& a, int4 q, float& lx
 #pragma unroll
       for (int j = 0; j < kNInterp; j++) {
         const float4* row = reinterpret_cast<const float4*>(a.phi + plane + iy[j] + a4);
-        const float4 f0 = __ldg(row), f1 = __ldg(row + 1), f2 = __ldg(row + 2);
-        const float v[12] = {f0.x - pc, f0.y - pc, f0.z - pc, f0.w - pc, f1.x - pc, f1.y - pc,
-                             f1.z - pc, f1.w - pc, f2.x - pc, f2.y - pc, f2.z - pc, f2.w - pc};
+        const float4 f0 = __ldg(row), f1 = __ldg(row + 1);
+        const float f8 = s == 3 ? __ldg(reinterpret_cast<const float*>(row + 2)) : pc;
+        const float v[9] = {f0.x - pc, f0.y - pc, f0.z - pc, f0.w - pc, f1.x - pc,
+                            f1.y - pc, f1.z - pc, f1.w - pc, f8 - pc};
         float rz = 0.f, rdz = 0.f;
 #pragma unroll
-        for (int m = 0; m < 12; m++) {
+        for (int m = 0; m < 9; m++) {
           rz = fmaf(ws[m], v[m], rz);
           rdz = fmaf(dws[m], v[m], rdz);
         }
