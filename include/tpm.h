@@ -63,6 +63,11 @@ extern "C" {
 #define TPM_SORT_PARITY 0
 #define TPM_SORT_FAST 1
 
+/* tpm_options.deterministic_deposit */
+#define TPM_DEPOSIT_FP32 0
+#define TPM_DEPOSIT_EXACT64 1
+#define TPM_DEPOSIT_FIXED32 2
+
 /*
  * Options.  The first block mirrors struct options (tigerpm/options.hpp:6-27)
  * field for field; tpm_options_init derives it as process_options does
@@ -102,11 +107,12 @@ typedef struct tpm_options {
   int deconv_order;    /* sinc^-p deconvolution; 0: assignment order (4/2/3) */
   int sort_mode;       /* TPM_SORT_*; default PARITY */
   int kahan;           /* 1: compensated per-target PP sums (default 1) */
-  int deterministic_deposit; /* 1: exact int64 fixed-point deposit, bit-reproducible;
-                              * 0 (default, faster): 26-bit fixed point in uint32,
-                              * bit-reproducible unless a mesh tile holds 16 or more
-                              * weight units at one point, which is then deposited
-                              * again with FP32 shared-memory atomics */
+  int deterministic_deposit; /* TPM_DEPOSIT_*: 0 (default) FP32 shared-memory
+                              * atomics; 1 exact int64 fixed point, bit-reproducible;
+                              * 2 26-bit fixed point in uint32 with integer adds
+                              * (fastest), bit-reproducible unless a mesh tile holds
+                              * 16 or more weight units at one point, which is then
+                              * deposited again with FP32 atomics */
   int fft;             /* TPM_FFT_*: 3-D transforms of gravity_long_compute */
   uint64_t seed;       /* synthetic-input seed carried for drivers */
   int fft_group;       /* x-planes per launch of the library FFT's z / y passes

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 ASSIGN_ID = {"cloud4": 0, "cic": 1, "tsc": 2}
 
 
-def device_phi(ps, grid, assign, rs_cells, typ, chain=3, exact=False, fft="auto"):
+def device_phi(ps, grid, assign, rs_cells, typ, chain=3, exact=0, fft="auto"):
     opts = make_options(round(ps.n ** (1 / 3)), grid, chain=chain, rs_cells=rs_cells, assign=assign,
                         deterministic_deposit=exact, fft=fft)
     with TigerPM(opts, ps.n) as t:
@@ -29,7 +29,7 @@ def device_phi(ps, grid, assign, rs_cells, typ, chain=3, exact=False, fft="auto"
 
 @pytest.mark.parametrize("assign", ["cloud4", "cic", "tsc"])
 @pytest.mark.parametrize("grid,n_side", [(32, 24), (30, 20), (45, 16), (200, 40)])
-@pytest.mark.parametrize("exact", [False, True])
+@pytest.mark.parametrize("exact", [0, 1, 2])
 def test_phi_matches_oracle(assign, grid, n_side, exact):
     ps = particle_set("uniform", n_side, 3)
     for typ in (GRAVITY_LONG_PME, GRAVITY_LONG_PM):
@@ -48,14 +48,14 @@ def test_deposit_mass_and_determinism():
     assert abs(float(np.mean(a.astype(np.float64)))) < 1e-4 * float(np.abs(a).max())
 
 
-def test_default_deposit_is_bit_reproducible():
-    """The default deposit accumulates 26-bit fixed point with integer adds:
-    repeated runs give identical bits, and phi agrees with the exact int64
-    deposit."""
+def test_fixed32_deposit_is_bit_reproducible():
+    """deterministic_deposit = 2 accumulates 26-bit fixed point with integer
+    adds: repeated runs give identical bits, and phi agrees with the exact
+    int64 deposit."""
     ps = particle_set("uniform", 24, 5)
-    a, _ = device_phi(ps, 32, "cloud4", 1.0, GRAVITY_LONG_PME)
-    b, _ = device_phi(ps, 32, "cloud4", 1.0, GRAVITY_LONG_PME)
-    c, _ = device_phi(ps, 32, "cloud4", 1.0, GRAVITY_LONG_PME, exact=True)
+    a, _ = device_phi(ps, 32, "cloud4", 1.0, GRAVITY_LONG_PME, exact=2)
+    b, _ = device_phi(ps, 32, "cloud4", 1.0, GRAVITY_LONG_PME, exact=2)
+    c, _ = device_phi(ps, 32, "cloud4", 1.0, GRAVITY_LONG_PME, exact=1)
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     assert rel_rms(a, c) < 1e-6, rel_rms(a, c)
 
@@ -63,14 +63,15 @@ def test_default_deposit_is_bit_reproducible():
 @pytest.mark.parametrize("assign", ["cloud4", "cic", "tsc"])
 def test_dense_clump_deposit_matches_oracle(assign):
     """2,000 particles inside one quarter mesh cell put hundreds of weight
-    units on a few points: the fixed-point tiles there overflow their range
-    and are deposited again in FP32; phi still matches the oracle."""
+    units on a few points: with deterministic_deposit = 2 the fixed-point
+    tiles there overflow their range and are deposited again in FP32; phi
+    matches the oracle in every mode."""
     ps = particle_set("uniform", 16, 7)
     g = np.random.default_rng(3)
     k = 2000
     for arr in (ps.x, ps.y, ps.z):
         arr[:k] = np.uint32(1 << 31) + g.integers(0, 1 << 25, k).astype(np.uint32)
-    for exact in (False, True):
+    for exact in (0, 1, 2):
         phi, (x, y, z) = device_phi(ps, 32, assign, 1.25, GRAVITY_LONG_PME, exact=exact)
         ref = O.gravity_long(32, 1.25, ASSIGN_ID[assign], x, y, z, pme=GRAVITY_LONG_PME)
         assert rel_rms(phi, ref) < 2e-6, (assign, exact, rel_rms(phi, ref))

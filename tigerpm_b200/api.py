@@ -75,11 +75,12 @@ def process_options(argv) -> Options:
 
 def make_options(n_side: int, grid: int, chain: int | None = None, rs_cells: float = 1.0,
                  rcut_over_rs: float = 0.0, assign: str = "cloud4", sort: str = "parity",
-                 kahan: bool = True, GM: float = 1.0, deterministic_deposit: bool = False,
+                 kahan: bool = True, GM: float = 1.0, deterministic_deposit: bool | int = False,
                  fft: str = "auto") -> Options:
     """Options for a box of n_side^3 particles on a grid^3 mesh.  chain=None
     picks the largest chain mesh whose cells are at least the cutoff wide
-    (or rcut = 4.5 rs wide when there is no cutoff)."""
+    (or rcut = 4.5 rs wide when there is no cutoff).  deterministic_deposit:
+    False / 0 FP32 atomics, True / 1 exact int64, 2 26-bit fixed point."""
     o = options_for(n_side, 1, 1)
     o.four_dim = grid
     o.parts_o_four = 1
@@ -92,7 +93,7 @@ def make_options(n_side: int, grid: int, chain: int | None = None, rs_cells: flo
     o.assign = _lib.ASSIGN[assign]
     o.sort_mode = _lib.SORT[sort]
     o.kahan = 1 if kahan else 0
-    o.deterministic_deposit = 1 if deterministic_deposit else 0
+    o.deterministic_deposit = int(deterministic_deposit)
     o.fft = _lib.FFT[fft]
     o.GM = GM
     return o

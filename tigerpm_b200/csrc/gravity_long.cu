@@ -13,11 +13,11 @@
 //    can reach it (particles are already in chain-cell order), compacts the
 //    ones that reach it into a shared list and accumulates their weights in
 //    shared memory; each grid point is written once, with no global atomics
-//    and no zeroing pass.  Accumulation is 26-bit fixed point with native
-//    32-bit shared integer adds by default (a tile that could overflow is
-//    deposited again with FP32 atomics), or (deterministic_deposit) exact
-//    40-bit fixed point in int64; integer sums are bit-for-bit reproducible
-//    whatever the thread order.
+//    and no zeroing pass.  Accumulation is FP32 shared atomics by default;
+//    deterministic_deposit selects exact 40-bit fixed point in int64, or
+//    26-bit fixed point with native 32-bit shared integer adds (a tile that
+//    could overflow is deposited again with FP32 atomics); integer sums are
+//    bit-for-bit reproducible whatever the thread order.
 //  * FFT: the library's own five-pass transforms (fft3d.cu) for meshes of
 //    the form 2^a 3^b 5^c that are multiples of 16, else (or with fft =
 //    cufft) cuFFT r2c / c2r around k_green; each timed as its own stages.
@@ -96,15 +96,15 @@ struct DepositArgs {
 };
 
 // Accumulator of one tile point.
-//  kDepI32 (default): 26-bit fixed point in uint32 with the native shared
-//    integer add; sums are order independent (bit-reproducible).  Weights
+//  kDepF32 (default): FP32 shared atomics (compare-and-swap loops; the
+//    rounding depends on the order in which threads reach a point).
+//  kDepI32 (TPM_DEPOSIT_FIXED32): 26-bit fixed point in uint32 with the
+//    native shared integer add; sums are order independent.  Weights
 //    are at most 1, so an add never carries a point past 2^32 without some
 //    earlier value at or above 2^30: every add returns the old value, and a
 //    tile where any old value reached 2^30 (16 weight units at one point) is
 //    deposited again with kDepF32.
-//  kDepI64 (deterministic_deposit): exact 40-bit fixed point in int64.
-//  kDepF32: FP32 shared atomics (compare-and-swap loops; the rounding
-//    depends on the order in which threads reach a point).
+//  kDepI64 (TPM_DEPOSIT_EXACT64): exact 40-bit fixed point in int64.
 constexpr int kDepF32 = 0, kDepI64 = 1, kDepI32 = 2;
 constexpr int kDep32FracBits = 26;
 template <int M>
@@ -506,11 +506,14 @@ int gravity_long(tpm_ctx* c, int type) {
   int rc;
   // tile edge: 24 points on large meshes (fewer redundant particle visits),
   // 16 / 8 on smaller ones; exact (int64) tiles of 24^3 would need 110 KB.
-  if (c->opt.deterministic_deposit) {
+  if (c->opt.deterministic_deposit == TPM_DEPOSIT_EXACT64) {
     rc = N >= 128 ? launch_deposit_T<16, kDepI64>(c, a) : launch_deposit_T<8, kDepI64>(c, a);
-  } else {
+  } else if (c->opt.deterministic_deposit == TPM_DEPOSIT_FIXED32) {
     rc = N >= 192 ? launch_deposit_T<24, kDepI32>(c, a)
                   : (N >= 64 ? launch_deposit_T<16, kDepI32>(c, a) : launch_deposit_T<8, kDepI32>(c, a));
+  } else {
+    rc = N >= 192 ? launch_deposit_T<24, kDepF32>(c, a)
+                  : (N >= 64 ? launch_deposit_T<16, kDepF32>(c, a) : launch_deposit_T<8, kDepF32>(c, a));
   }
   if (rc) return rc;
   stage_end(c, kStDeposit);

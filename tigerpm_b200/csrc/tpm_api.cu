@@ -78,6 +78,8 @@ int derive(tpm_ctx* c) {
   if (o.assign < 0 || o.assign > 2) return fail(TPM_ERR_INVALID, "assign must be cloud4, cic or tsc");
   if (o.sort_mode < 0 || o.sort_mode > 1) return fail(TPM_ERR_INVALID, "sort_mode must be parity or fast");
   if (o.fft < 0 || o.fft > 2) return fail(TPM_ERR_INVALID, "fft must be auto, cufft or block");
+  if (o.deterministic_deposit < TPM_DEPOSIT_FP32 || o.deterministic_deposit > TPM_DEPOSIT_FIXED32)
+    return fail(TPM_ERR_INVALID, "deterministic_deposit must be 0 (fp32), 1 (exact64) or 2 (fixed32)");
   c->N = o.four_dim;
   c->C = o.chain_dim;
   c->rs_box = o.rs;
