@@ -543,8 +543,9 @@ struct LineCfg {
   // 512 (128 registers) from 28 values per lane up
   static constexpr int kMinBlocks = (E >= 28 ? 2 : 3) * 256 / kThreads;
   static constexpr size_t kSmem = sizeof(float2) * ((size_t)N + (size_t)kLineCols * LS);
-  // the x pass holds the stage tables of both radix orders
-  static constexpr size_t kSmemX = kSmem + sizeof(float2) * (size_t)N;
+  // the x pass holds the stage tables of both radix orders and the x axis's
+  // Green's-function and k^2 tables (read from shared memory, not L1)
+  static constexpr size_t kSmemX = kSmem + sizeof(float2) * (size_t)N + sizeof(float) * 2 * (size_t)N;
   static_assert(P.ns >= 1 && P.ns <= 6, "no line plan for this N");
 };
 
@@ -775,6 +776,12 @@ __global__ void __launch_bounds__(LineCfg<N>::kThreads, LineCfg<N>::kMinBlocks)
   float2* s_twr = lsm + N;
   float2* lines = lsm + 2 * N;
   for (int i = threadIdx.x; i < 2 * N; i += L::kThreads) s_tw[i] = __ldg(tw + i);
+  float* s_gt = reinterpret_cast<float*>(lines + kLineCols * L::LS);
+  float* s_k2 = s_gt + N;
+  for (int i = threadIdx.x; i < N; i += L::kThreads) {
+    s_gt[i] = __ldg(gt + i);
+    s_k2[i] = __ldg(k2tab + i);
+  }
   const int li = threadIdx.x / L::TL, lane = threadIdx.x - li * L::TL;
   float2* line = lines + li * L::LS;
   const int per_y = Sz / kLineCols;
@@ -799,8 +806,8 @@ __global__ void __launch_bounds__(LineCfg<N>::kThreads, LineCfg<N>::kMinBlocks)
 #pragma unroll
     for (int r = 0; r < RL; r++) {
       const int n = lane + L::TL * b + r * (N / RL);
-      const float k2 = __ldg(k2tab + n) + k2yz;
-      const float g = k2 > 0.0f ? -(__ldg(gt + n) * gyz) * __frcp_rn(k2) * norm : 0.0f;
+      const float k2 = s_k2[n] + k2yz;
+      const float g = k2 > 0.0f ? -(s_gt[n] * gyz) * __frcp_rn(k2) * norm : 0.0f;
       v[b * RL + r] = make_float2(v[b * RL + r].x * g, v[b * RL + r].y * g);
     }
   // The inverse recomputes its addresses: with the lane index passed through
