@@ -618,7 +618,9 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
           const unsigned b = __ballot_sync(0xffffffffu, keep);
           if (keep) buf[cnt + __popc(b & lt)] = s;
           cnt += __popc(b);
-          if (cnt >= 32) {
+          // the count is the same in every lane; a vote makes the branch
+          // warp-uniform for the compiler (no reconvergence region)
+          if (__all_sync(0xffffffffu, cnt >= 32)) {
             __syncwarp();
 #pragma unroll
             for (int k = 0; k < 32; k += 4) {
