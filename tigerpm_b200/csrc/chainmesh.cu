@@ -252,6 +252,17 @@ __device__ __forceinline__ int left_flag(const Node& nd, uint32_t k, int C) {
   return c < nd.mid ? 1 : 0;
 }
 
+// Four consecutive int32 entries from position p (a multiple of 4, so the
+// 16-byte load is aligned) when all four are below n; else one by one.
+__device__ __forceinline__ int4 load4(const int32_t* __restrict__ a, int64_t p, int64_t n) {
+  if (p + 4 <= n) return *reinterpret_cast<const int4*>(a + p);
+  int4 r = make_int4(0, 0, 0, 0);
+  if (p < n) r.x = a[p];
+  if (p + 1 < n) r.y = a[p + 1];
+  if (p + 2 < n) r.z = a[p + 2];
+  return r;
+}
+
 // Node lookups are cached while consecutive positions share a final cell
 // (cells hold many particles), which removes most dependent loads.
 struct NodeCache {
@@ -277,8 +288,10 @@ __device__ __forceinline__ unsigned long long pack_status(unsigned stamp, unsign
 // look-back; tiles are taken in launch order through an atomic counter, so
 // every predecessor a tile waits on is already running).  The look-back is
 // done by one warp, 32 predecessor tiles at a time; its spin is bounded: on
-// expiry the tile records kErrTimeout and uses what it has summed.
-__global__ void __launch_bounds__(kScanThreads) k_level_scan(LevelArgs a, unsigned stamp, int* __restrict__ counter,
+// expiry the tile records kErrTimeout and uses what it has summed.  Cells,
+// keys and prefixes move 16 bytes per load / store; four resident blocks per
+// SM (32 registers) beat three at 40 registers without the bound.
+__global__ void __launch_bounds__(kScanThreads, 4) k_level_scan(LevelArgs a, unsigned stamp, int* __restrict__ counter,
                                                              unsigned long long* __restrict__ status,
                                                              int32_t* __restrict__ prefix, int* __restrict__ err) {
   __shared__ int warp_tot[32];
@@ -292,12 +305,20 @@ __global__ void __launch_bounds__(kScanThreads) k_level_scan(LevelArgs a, unsign
   int v[kScanItems];
   int s = 0;
   NodeCache cache;
+  static_assert(kScanItems % 4 == 0, "positions are read four at a time");
+  // cells and keys of the thread's positions, four at a time (16-byte loads)
 #pragma unroll
-  for (int k = 0; k < kScanItems; k++) {
-    const int64_t p = base + k;
-    v[k] = 0;
-    if (p < a.n) v[k] = left_flag(cache.get(a, a.cellof[p]), a.key[p], a.C);
-    s += v[k];
+  for (int k = 0; k < kScanItems; k += 4) {
+    const int4 c = load4(a.cellof, base + k, a.n);
+    const int4 q = load4(reinterpret_cast<const int32_t*>(a.key), base + k, a.n);
+    const int cof[4] = {c.x, c.y, c.z, c.w}, ky[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int64_t p = base + k + i;
+      v[k + i] = 0;
+      if (p < a.n) v[k + i] = left_flag(cache.get(a, cof[i]), (uint32_t)ky[i], a.C);
+      s += v[k + i];
+    }
   }
   const int off = block_exclusive_scan(s, warp_tot, &total);
   if (threadIdx.x < 32) {
@@ -344,11 +365,20 @@ __global__ void __launch_bounds__(kScanThreads) k_level_scan(LevelArgs a, unsign
   }
   __syncthreads();
   int run = excl_s + off;
+  int pr[kScanItems];
 #pragma unroll
   for (int k = 0; k < kScanItems; k++) {
-    const int64_t p = base + k;
-    if (p < a.n) prefix[p] = run;
+    pr[k] = run;
     run += v[k];
+  }
+  if (base + kScanItems <= a.n) {
+#pragma unroll
+    for (int k = 0; k < kScanItems; k += 4)
+      *reinterpret_cast<int4*>(prefix + base + k) = make_int4(pr[k], pr[k + 1], pr[k + 2], pr[k + 3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+      if (base + k < a.n) prefix[base + k] = pr[k];
   }
   if (base < a.n && base + kScanItems >= a.n) prefix[a.n] = run;  // the thread holding position n-1
 }
@@ -360,14 +390,19 @@ __global__ void __launch_bounds__(256) k_level_slots(LevelArgs a, const int32_t*
                                                      int32_t* __restrict__ slot) {
   const int64_t p0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 4;
   NodeCache cache;
+  const int4 c4 = load4(a.cellof, p0, a.n);
+  const int4 k4 = load4(reinterpret_cast<const int32_t*>(a.key), p0, a.n);
+  const int4 f4 = load4(prefix, p0, a.n);
+  const int cof[4] = {c4.x, c4.y, c4.z, c4.w}, ky[4] = {k4.x, k4.y, k4.z, k4.w};
+  const int pf[4] = {f4.x, f4.y, f4.z, f4.w};
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     const int64_t p = p0 + k;
     if (p >= a.n) return;
-    const Node& nd = cache.get(a, a.cellof[p]);
+    const Node& nd = cache.get(a, cof[k]);
     if (!nd.live || p < nd.pm) continue;
-    if (left_flag(nd, a.key[p], a.C)) {
-      const int32_t kk = prefix[nd.e] - prefix[p] - 1;  // flagged elements in (p, e)
+    if (left_flag(nd, (uint32_t)ky[k], a.C)) {
+      const int32_t kk = prefix[nd.e] - pf[k] - 1;  // flagged elements in (p, e)
       slot[nd.b + kk] = (int32_t)p;
     }
   }
@@ -380,14 +415,19 @@ __global__ void __launch_bounds__(256) k_level_swap(LevelArgs a, const int32_t* 
                                                     int32_t* __restrict__ idx) {
   const int64_t p0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 4;
   NodeCache cache;
+  // cells and prefixes are read-only here; keys are swapped by other
+  // threads (at right-part positions), so they are read one by one
+  const int4 c4 = load4(a.cellof, p0, a.n);
+  const int4 f4 = load4(prefix, p0, a.n);
+  const int cof[4] = {c4.x, c4.y, c4.z, c4.w}, pf[4] = {f4.x, f4.y, f4.z, f4.w};
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     const int64_t p = p0 + k;
     if (p >= a.n) return;
-    const Node& nd = cache.get(a, a.cellof[p]);
+    const Node& nd = cache.get(a, cof[k]);
     if (!nd.live || p >= nd.pm) continue;
     if (!left_flag(nd, key[p], a.C)) {
-      const int32_t kk = (int32_t)(p - nd.b) - (prefix[p] - prefix[nd.b]);  // unflagged in [b, p)
+      const int32_t kk = (int32_t)(p - nd.b) - (pf[k] - prefix[nd.b]);  // unflagged in [b, p)
       const int32_t q = slot[nd.b + kk];
       const uint32_t kp = key[p], kq = key[q];
       const int32_t ip = idx[p], iq = idx[q];
