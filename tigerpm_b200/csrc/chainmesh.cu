@@ -34,6 +34,12 @@ namespace {
 constexpr int kScanThreads = 512;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
+#ifndef TPM_LEVEL_PER
+#define TPM_LEVEL_PER 4
+#endif
+// consecutive positions per thread in the slot and swap passes (a multiple of 4)
+constexpr int kLevelPer = TPM_LEVEL_PER;
+static_assert(kLevelPer % 4 == 0, "positions are read four at a time");
 static_assert(kScanTile == kScanTileElems, "scan tiles must match the status and block-sum arrays");
 
 // Cell coordinate of raw position r along one axis: the largest m with
@@ -388,15 +394,20 @@ __global__ void __launch_bounds__(kScanThreads, 4) k_level_scan(LevelArgs a, uns
 // end of the node goes to slot[b + k].
 __global__ void __launch_bounds__(256) k_level_slots(LevelArgs a, const int32_t* __restrict__ prefix,
                                                      int32_t* __restrict__ slot) {
-  const int64_t p0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 4;
+  const int64_t p0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * kLevelPer;
   NodeCache cache;
-  const int4 c4 = load4(a.cellof, p0, a.n);
-  const int4 k4 = load4(reinterpret_cast<const int32_t*>(a.key), p0, a.n);
-  const int4 f4 = load4(prefix, p0, a.n);
-  const int cof[4] = {c4.x, c4.y, c4.z, c4.w}, ky[4] = {k4.x, k4.y, k4.z, k4.w};
-  const int pf[4] = {f4.x, f4.y, f4.z, f4.w};
+  int cof[kLevelPer], ky[kLevelPer], pf[kLevelPer];
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
+  for (int h = 0; h < kLevelPer; h += 4) {
+    const int4 c4 = load4(a.cellof, p0 + h, a.n);
+    const int4 k4 = load4(reinterpret_cast<const int32_t*>(a.key), p0 + h, a.n);
+    const int4 f4 = load4(prefix, p0 + h, a.n);
+    cof[h] = c4.x, cof[h + 1] = c4.y, cof[h + 2] = c4.z, cof[h + 3] = c4.w;
+    ky[h] = k4.x, ky[h + 1] = k4.y, ky[h + 2] = k4.z, ky[h + 3] = k4.w;
+    pf[h] = f4.x, pf[h + 1] = f4.y, pf[h + 2] = f4.z, pf[h + 3] = f4.w;
+  }
+#pragma unroll
+  for (int k = 0; k < kLevelPer; k++) {
     const int64_t p = p0 + k;
     if (p >= a.n) return;
     const Node& nd = cache.get(a, cof[k]);
@@ -413,15 +424,20 @@ __global__ void __launch_bounds__(256) k_level_slots(LevelArgs a, const int32_t*
 __global__ void __launch_bounds__(256) k_level_swap(LevelArgs a, const int32_t* __restrict__ prefix,
                                                     const int32_t* __restrict__ slot, uint32_t* __restrict__ key,
                                                     int32_t* __restrict__ idx) {
-  const int64_t p0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 4;
+  const int64_t p0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * kLevelPer;
   NodeCache cache;
   // cells and prefixes are read-only here; keys are swapped by other
   // threads (at right-part positions), so they are read one by one
-  const int4 c4 = load4(a.cellof, p0, a.n);
-  const int4 f4 = load4(prefix, p0, a.n);
-  const int cof[4] = {c4.x, c4.y, c4.z, c4.w}, pf[4] = {f4.x, f4.y, f4.z, f4.w};
+  int cof[kLevelPer], pf[kLevelPer];
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
+  for (int h = 0; h < kLevelPer; h += 4) {
+    const int4 c4 = load4(a.cellof, p0 + h, a.n);
+    const int4 f4 = load4(prefix, p0 + h, a.n);
+    cof[h] = c4.x, cof[h + 1] = c4.y, cof[h + 2] = c4.z, cof[h + 3] = c4.w;
+    pf[h] = f4.x, pf[h + 1] = f4.y, pf[h + 2] = f4.z, pf[h + 3] = f4.w;
+  }
+#pragma unroll
+  for (int k = 0; k < kLevelPer; k++) {
     const int64_t p = p0 + k;
     if (p >= a.n) return;
     const Node& nd = cache.get(a, cof[k]);
@@ -595,7 +611,7 @@ int chainmesh_sort(tpm_ctx* c) {
       int* counters = c->cell_count;  // reused: C^3 + 1 >= levels ints after the scan above
       unsigned long long* status = c->scan_status;
       TPM_CUDA_TRY(cudaMemsetAsync(counters, 0, sizeof(int) * (levels + 1), s));
-      const int nq = ceil_div(n, 4);
+      const int nq = ceil_div(n, kLevelPer);
       for (int l = 0; l < levels; l++) {
         LevelArgs a{n, C, l, c->cellof, c->key, c->cell_begin, c->tree, c->depth1d};
         const unsigned stamp = (unsigned)(++c->scan_stamp & 0x3fffffff);
