@@ -72,11 +72,12 @@ struct KickArgs {
   int first_call;
   int kahan;
   float GM, eta, t0, scale, hsoft;
-  // pair-loop lengths are in units of 2 r_s (see PairK)
+  // pair-loop lengths are in units of u = 2 r_s / sqrt(log2 e) (see pair())
   float inv2rs;  // 1 / (2 r_s), box units
-  float lscale;  // 2^-32 / (2 r_s): fixed32 offset -> scaled length
-  float h2;      // (hsoft / 2 r_s)^2
-  float rcut2;   // (r_cut / 2 r_s)^2, or infinity without a cutoff
+  float lscale;  // 2^-32 / u: fixed32 offset -> scaled length
+  float h2;      // (hsoft / u)^2
+  float rcut2;   // (r_cut / u)^2, or infinity without a cutoff
+  float wlen;    // the box length / u (minimum-image fold, chain_dim = 3)
 };
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
@@ -351,66 +352,101 @@ __global__ void __launch_bounds__(128) k_interp_tile(KickArgs a, int maxw) {
   }
 }
 
-// One source against one sink (src/kick_pme.cu:285-314).  WRAP folds the
-// offset to the minimum image, as the reference's int32 difference does; it
-// is needed only when chain_dim = 3, where the 27 cells span the whole box
-// and an offset from the cell centre can exceed half the box.
-// Pair constants that stay in registers through the pair loop.  Lengths in
-// the pair loop are in units of 2 r_s, so that the erfc argument
-// x0 = r / (2 r_s) is r itself and the A&S and exp constants are literals:
-// rcut2 and h2 are (r_cut / 2 r_s)^2 and (h / 2 r_s)^2; wrap_len is the box
-// length in those units (minimum-image fold, chain_dim = 3 only).
+// Pair constants that stay in registers through the pair loop, in the pair
+// loop's length unit u (below): rcut2 and h2 are (r_cut / u)^2 and (h / u)^2;
+// wrap_len is the box length in u (minimum-image fold, chain_dim = 3 only).
+constexpr float kLog2e = 1.4426950408889634f, kSqrtLog2e = 1.2011224087864498f;
 struct PairK {
   float rcut2, h2, wrap_len;
 };
 
-// One source against one sink (src/kick_pme.cu:285-314).  WRAP folds the
-// offset to the minimum image, as the reference's int32 difference does; it
-// is needed only when chain_dim = 3, where the 27 cells span the whole box
-// and an offset from the cell centre can exceed half the box.  Sums are in
-// the scaled units: force x 1/(2 r_s)^2, potential x 1/(2 r_s).
-// CONVERGED: every lane of the warp calls it together; the softened branch
-// is then taken only when some lane of the warp needs it (a warp vote), and
-// inside it each lane selects its own result.
-template <bool WRAP, bool CONVERGED = false>
-__device__ __forceinline__ void pair(const PairK& k, float dx, float dy, float dz, float& gx, float& gy, float& gz,
-                                     float& ph) {
+// One source against one sink (src/kick_pme.cu:285-314), in three parts:
+// the separation and the erfc-split terms, the softened kernel, and the
+// sums.  WRAP folds the offset to the minimum image, as the reference's
+// int32 difference does; it is needed only when chain_dim = 3, where the 27
+// cells span the whole box and an offset from the cell centre can exceed
+// half the box.
+//
+// Lengths are in units of u = 2 r_s / s with s = sqrt(log2 e) (the caller
+// scales offsets by 1 / u): r2 = log2(e) x0^2 for x0 = r / (2 r_s), so
+// exp(-x0^2) = 2^-r2 takes no multiply.  With x0 = r / s the A&S and
+// 2/sqrt(pi) constants are divided by s, and the sums come out as force x
+// u^2 and potential x u; the caller multiplies them back.  The softened
+// terms are homogeneous in r and h, so their formulas are unchanged.
+template <bool WRAP>
+__device__ __forceinline__ void pair_terms(const PairK& k, float& dx, float& dy, float& dz, float& r2, float& rinv3,
+                                           float& q) {
   if (WRAP) {
     const float inv = 1.0f / k.wrap_len;
     dx -= rintf(dx * inv) * k.wrap_len;
     dy -= rintf(dy * inv) * k.wrap_len;
     dz -= rintf(dz * inv) * k.wrap_len;
   }
-  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   // Pairs beyond the cutoff take r^2 = 1e30: 1/r, erfc and exp(-x^2) then
   // vanish and the pair adds exactly 0, without a mask on the results.
   // Pairs at r <= h (the sink itself included, r = 0) take the softened
-  // branch below, which replaces every term the lines before it form.
+  // kernel, which replaces every term formed here.
   const float r2c = r2 < k.rcut2 ? r2 : 1e30f;
   const float rinv = rsqrt_approx(r2c);
   const float r = r2c * rinv;
-  // A&S 7.1.26 erfc(x0) with x0 = r; exp(-x0^2) = 2^(-log2(e) r^2)
-  const float t = rcp_approx(fmaf(0.3275911f, r, 1.0f));
-  const float e = ex2_approx(-1.4426950408889634f * r2c);
+  // A&S 7.1.26 erfc(x0), t = 1 / (1 + 0.3275911 x0) with x0 = r / s
+  const float t = rcp_approx(fmaf(0.2727374808792225f, r, 1.0f));
+  const float e = ex2_approx(-r2c);
   const float poly =
       t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f), 0.254829592f);
   // potential term erfc / r, and the force term
-  // (erfc + (2/sqrt(pi)) r e) / r^3 = (erfc / r + (2/sqrt(pi)) e) / r^2
-  float q = poly * e * rinv;
-  float rinv3 = fmaf(1.1283791670955126f, e, q) * (rinv * rinv);
-  const bool soft = r2 <= k.h2;  // softened Newtonian kernel inside hsoft (rare)
-  if (CONVERGED ? __any_sync(0xffffffffu, soft) : soft) {
-    const float hinv = rsqrtf(k.h2);
-    const float q2 = r2 * hinv * hinv;
-    const float s3 = fmaf(fmaf(15.0f / 8.0f, q2, -21.0f / 4.0f), q2, 35.0f / 8.0f) * (hinv * hinv * hinv);
-    const float s1 = fmaf(fmaf(fmaf(-5.0f / 16.0f, q2, 21.0f / 16.0f), q2, -35.0f / 16.0f), q2, 35.0f / 16.0f) * hinv;
-    rinv3 = soft ? s3 : rinv3;
-    q = soft ? s1 : q;
-  }
+  // (erfc + (2/sqrt(pi)) x0 e) / r^3 = (erfc / r + (2/sqrt(pi)) e / s) / r^2
+  q = poly * e * rinv;
+  rinv3 = fmaf(0.9394372786996513f, e, q) * (rinv * rinv);
+}
+
+// The softened Newtonian kernel where r <= h (rare), selected per lane.
+__device__ __forceinline__ void soften(const PairK& k, float r2, float& rinv3, float& q) {
+  const bool soft = r2 <= k.h2;
+  const float hinv = rsqrtf(k.h2);
+  const float q2 = r2 * hinv * hinv;
+  const float s3 = fmaf(fmaf(15.0f / 8.0f, q2, -21.0f / 4.0f), q2, 35.0f / 8.0f) * (hinv * hinv * hinv);
+  const float s1 = fmaf(fmaf(fmaf(-5.0f / 16.0f, q2, 21.0f / 16.0f), q2, -35.0f / 16.0f), q2, 35.0f / 16.0f) * hinv;
+  rinv3 = soft ? s3 : rinv3;
+  q = soft ? s1 : q;
+}
+
+__device__ __forceinline__ void add_pair(float dx, float dy, float dz, float rinv3, float q, float& gx, float& gy,
+                                         float& gz, float& ph) {
   gx = fmaf(-dx, rinv3, gx);
   gy = fmaf(-dy, rinv3, gy);
   gz = fmaf(-dz, rinv3, gz);
   ph -= q;
+}
+
+// One pair, the softened kernel behind a per-lane branch (any caller).
+template <bool WRAP>
+__device__ __forceinline__ void pair(const PairK& k, float dx, float dy, float dz, float& gx, float& gy, float& gz,
+                                     float& ph) {
+  float r2, rinv3, q;
+  pair_terms<WRAP>(k, dx, dy, dz, r2, rinv3, q);
+  if (r2 <= k.h2) soften(k, r2, rinv3, q);
+  add_pair(dx, dy, dz, rinv3, q, gx, gy, gz, ph);
+}
+
+// Two pairs of one sink, evaluated by every lane of the warp together: the
+// softened kernel is entered on one warp vote for both (a uniform branch),
+// and the sums take the first pair, then the second.
+template <bool WRAP>
+__device__ __forceinline__ void pair2(const PairK& k, const float4& sp, const float4& u0, const float4& u1, float& gx,
+                                      float& gy, float& gz, float& ph) {
+  float dx0 = sp.x - u0.x, dy0 = sp.y - u0.y, dz0 = sp.z - u0.z;
+  float dx1 = sp.x - u1.x, dy1 = sp.y - u1.y, dz1 = sp.z - u1.z;
+  float r20, rinv30, q0, r21, rinv31, q1;
+  pair_terms<WRAP>(k, dx0, dy0, dz0, r20, rinv30, q0);
+  pair_terms<WRAP>(k, dx1, dy1, dz1, r21, rinv31, q1);
+  if (__any_sync(0xffffffffu, r20 <= k.h2 || r21 <= k.h2)) {
+    soften(k, r20, rinv30, q0);
+    soften(k, r21, rinv31, q1);
+  }
+  add_pair(dx0, dy0, dz0, rinv30, q0, gx, gy, gz, ph);
+  add_pair(dx1, dy1, dz1, rinv31, q1, gx, gy, gz, ph);
 }
 
 // Offset a - b of two fixed32 coordinates (the reference's int32 wrap-around
@@ -479,12 +515,14 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int t8 = lane & 7, ph = lane >> 3;
   const float Cf = (float)C;
-  // culling works on unwrapped offsets; without it every source is kept
-  const float keep2 = !WRAP && a.rcut2 < INFINITY ? a.rcut2 : INFINITY;
   unsigned lt;  // lanes below this one
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+  // offsets, cutoff and softening length in units of 2 r_s / sqrt(log2 e)
+  // (see pair())
   const float sc = a.lscale;
-  const PairK pk{a.rcut2, a.h2, a.inv2rs};
+  const PairK pk{a.rcut2, a.h2, a.wlen};
+  // culling works on unwrapped offsets; without it every source is kept
+  const float keep2 = !WRAP && a.rcut2 < INFINITY ? a.rcut2 : INFINITY;
   if (tid == 0) {
     int nr = 0, tot = 0;
     for (int dz = -1; dz <= 1; dz++) {
@@ -623,11 +661,10 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
           if (__all_sync(0xffffffffu, cnt >= 32)) {
             __syncwarp();
 #pragma unroll
-            for (int k = 0; k < 32; k += 4) {
+            for (int k = 0; k < 32; k += 8) {
               // lanes without a sink (a partial group) hold a copy of the
               // group's first sink; their sums are never committed
-              const float4 u = buf[k + ph];
-              pair<WRAP, true>(pk, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
+              pair2<WRAP>(pk, sp, buf[k + ph], buf[k + 4 + ph], px, py, pz, pp);
             }
             __syncwarp();
             if (lane < cnt - 32) buf[lane] = buf[32 + lane];
@@ -636,18 +673,20 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
           }
         }
         __syncwarp();
-        for (int k = 0; k < cnt; k += 4) {
-          if (WRAP) {
+        if (WRAP) {
+          for (int k = 0; k < cnt; k += 4) {
             if (k + ph < cnt && mysink) {
               const float4 u = buf[k + ph];
               pair<WRAP>(pk, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
             }
-          } else {
-            // past the count a lane takes a source 1e18 units away: beyond
-            // any cutoff, its terms are exactly 0 (no minimum-image fold here)
-            const float4 u = k + ph < cnt ? buf[k + ph] : make_float4(1e18f, 1e18f, 1e18f, 0.f);
-            pair<WRAP, true>(pk, sp.x - u.x, sp.y - u.y, sp.z - u.z, px, py, pz, pp);
           }
+        } else {
+          // past the count a lane takes a source 1e18 units away: beyond any
+          // cutoff, its terms are exactly 0 (no minimum-image fold here)
+          const float4 far = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+          for (int k = 0; k < cnt; k += 8)
+            pair2<WRAP>(pk, sp, k + ph < cnt ? buf[k + ph] : far, k + 4 + ph < cnt ? buf[k + 4 + ph] : far, px, py,
+                        pz, pp);
         }
         __syncwarp();
         // fold the four source phases (fixed order), lanes 0..7 hold the group's sums
@@ -681,11 +720,11 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
       const float lx = a.gx[i], ly = a.gy[i], lz = a.gz[i], lp = a.pot[i];  // from k_interp_long
       const float* A = acc + e * 8;
       // pair sums back from units of 2 r_s: force x (1/2r_s)^2, potential x 1/2r_s
-      const float fs = a.inv2rs * a.inv2rs;
+      const float fs = a.inv2rs * a.inv2rs * kLog2e;
       const float g0 = fmaf(A[0] - A[4], fs, lx) * a.GM;
       const float g1 = fmaf(A[1] - A[5], fs, ly) * a.GM;
       const float g2 = fmaf(A[2] - A[6], fs, lz) * a.GM;
-      const float phi = fmaf(A[3] - A[7], a.inv2rs, lp) * a.GM;
+      const float phi = fmaf(A[3] - A[7], a.inv2rs * kSqrtLog2e, lp) * a.GM;
       a.gx[i] = g0;
       a.gy[i] = g1;
       a.gz[i] = g2;
@@ -1003,9 +1042,12 @@ KickArgs make_args(tpm_ctx* c, const int b[3], const int e[3], int min_rung, dou
   a.hsoft = (float)c->opt.hsoft;
   const double inv2rs = 0.5 / c->rs_box;
   a.inv2rs = (float)inv2rs;
-  a.lscale = (float)(inv2rs * 2.3283064365386963e-10);
-  a.h2 = (float)((c->opt.hsoft * inv2rs) * (c->opt.hsoft * inv2rs));
-  a.rcut2 = c->rcut_box > 0 ? (float)((c->rcut_box * inv2rs) * (c->rcut_box * inv2rs)) : INFINITY;
+  // lengths in u = 2 r_s / sqrt(log2 e), formed in FP64
+  const double su = inv2rs * std::sqrt(1.4426950408889634);
+  a.lscale = (float)(su * 2.3283064365386963e-10);
+  a.h2 = (float)((c->opt.hsoft * su) * (c->opt.hsoft * su));
+  a.rcut2 = c->rcut_box > 0 ? (float)((c->rcut_box * su) * (c->rcut_box * su)) : INFINITY;
+  a.wlen = (float)su;
   return a;
 }
 
