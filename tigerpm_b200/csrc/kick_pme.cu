@@ -1,4 +1,4 @@
-// kick_pme.cu -- fused long-range interpolation + short-range PP + rung kick.
+// kick_pme.cu -- long-range interpolation, short-range PP and the rung kick.
 //
 // Reference: kick_pme_kernel (src/kick_pme.cu:128-357) behind the host
 // staging of kick_pme (src/kick_pme.cu:390-621).  Per sink: the 6-point
@@ -12,20 +12,25 @@
 //  * No host staging: particles are already in chain-cell order on the device
 //    and the 27 neighbours of a cell are 9 contiguous (z, y) rows of three x
 //    cells (two runs where x wraps), read straight from cell offsets.
-//  * One block per sink cell.  Source tiles are staged in shared memory as
-//    float offsets from the sink cell centre: the int32 wrap-around
-//    difference (the reference's periodic minimum image) is taken once per
-//    source per block, so the pair loop is pure FP32 (FADD for dx).
-//  * Culling: the cell's sinks (up to 256 at a time) are ordered by a 9-bit
+//  * The interpolation is its own kernel (one block per chain cell), run just
+//    before the pair kernel; its results stay in L2 for the kick.
+//  * Pair kernel, one block per sink cell.  Sources are staged in shared
+//    memory as float offsets from the sink cell centre: the int32
+//    wrap-around difference (the reference's periodic minimum image) is taken
+//    once per source per block, so the pair loop is pure FP32.
+//  * Culling: the cell's sinks (up to 256 per pass) are ordered by a 9-bit
 //    Morton key of their position inside the cell (a deterministic bitonic
-//    sort in shared memory), so each warp holds 32 spatially compact sinks.
-//    Each warp compacts every staged source tile to the sources within the
-//    cutoff of its sinks' bounding box (ballot + popc into a per-warp index
-//    list) and evaluates only those; the exact r < rcut test stays per pair.
-//  * Pair kernel: rsqrt / rcp / ex2 approximations (MUFU) for 1/r, the A&S
-//    rational and exp(-x^2); an optional cutoff masks pairs beyond rcut.
-//  * Precision: FP32 pair terms summed in chunks of 64 sources, chunk sums
-//    added with Kahan compensation per target (kahan option).
+//    sort) and cut into groups of 8; a warp keeps the sources within the
+//    cutoff of a group's bounding box (ballot + popc) in a float4 buffer, and
+//    lanes (8 sinks x 4 source phases) evaluate it 32 sources at a time,
+//    every lane together: the flush is a warp-uniform branch, pairs go two at
+//    a time with one warp vote for the softened kernel.
+//  * Pair terms: rsqrt / rcp / ex2 approximations (MUFU) for 1/r, the A&S
+//    rational and exp(-x^2), with lengths in units of 2 r_s / sqrt(log2 e)
+//    so that exp(-x0^2) = 2^-r2; an optional cutoff zeroes pairs beyond it.
+//  * Precision: FP32 pair terms, per-lane FP32 partial sums folded in a fixed
+//    order, added per target with Kahan compensation across staged chunks
+//    (kahan option).
 #include "tpm_internal.cuh"
 
 #include <algorithm>
@@ -39,8 +44,9 @@ constexpr int kKickThreads = 256;
 // (256^3 particles, 64^3 cells): 64 registers (4 resident 256-thread blocks
 // per SM), a staged chunk of half the mean 27-cell neighbourhood and a sink
 // pass of the power of two >= the mean cell give 8 resident 128-thread
-// blocks and the shortest kick (18.8 ms; 26.9 ms at 80 registers and 4 blocks,
-// 20.9 ms at 48 or 40 registers, where the pair loop loses ILP).
+// blocks and the shortest kick (at the time 18.8 ms against 26.9 ms at 80
+// registers and 4 blocks, 20.9 ms at 48 or 40 registers, where the pair
+// loop loses ILP).
 #ifndef TPM_KICK_MINB
 #define TPM_KICK_MINB 4  // resident 256-thread blocks per SM the register budget targets
 #endif
