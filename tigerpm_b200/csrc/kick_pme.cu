@@ -440,7 +440,7 @@ __device__ __forceinline__ void pair(const PairK& k, float dx, float dy, float d
 // softened kernel is entered on one warp vote for both (a uniform branch),
 // and the sums take the first pair, then the second.
 template <bool WRAP>
-__device__ __forceinline__ void pair2(const PairK& k, const float4& sp, const float4& u0, const float4& u1, float& gx,
+__device__ __forceinline__ void pair2(const PairK& k, const float4& sp, const float4 u0, const float4 u1, float& gx,
                                       float& gy, float& gz, float& ph) {
   float dx0 = sp.x - u0.x, dy0 = sp.y - u0.y, dz0 = sp.z - u0.z;
   float dx1 = sp.x - u1.x, dy1 = sp.y - u1.y, dz1 = sp.z - u1.z;
@@ -690,9 +690,11 @@ __device__ __forceinline__ void kick_cell(const KickArgs& a, int cx, int cy, int
           // past the count a lane takes a source 1e18 units away: beyond any
           // cutoff, its terms are exactly 0 (no minimum-image fold here)
           const float4 far = make_float4(1e18f, 1e18f, 1e18f, 0.f);
-          for (int k = 0; k < cnt; k += 8)
-            pair2<WRAP>(pk, sp, k + ph < cnt ? buf[k + ph] : far, k + 4 + ph < cnt ? buf[k + 4 + ph] : far, px, py,
-                        pz, pp);
+          for (int k = 0; k < cnt; k += 8) {
+            const float4 u0 = k + ph < cnt ? buf[k + ph] : far;
+            const float4 u1 = k + 4 + ph < cnt ? buf[k + 4 + ph] : far;
+            pair2<WRAP>(pk, sp, u0, u1, px, py, pz, pp);
+          }
         }
         __syncwarp();
         // fold the four source phases (fixed order), lanes 0..7 hold the group's sums
