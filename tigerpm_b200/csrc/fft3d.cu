@@ -542,6 +542,10 @@ struct LineCfg {
   // resident threads per SM the register budget targets: 768 (85 registers),
   // 512 (128 registers) from 28 values per lane up
   static constexpr int kMinBlocks = (E >= 28 ? 2 : 3) * 256 / kThreads;
+  // the x pass (two transforms and the Green's function) from 24 values per
+  // lane: 2 blocks (128 registers, no spills) beat 3 that spill
+  // (768^3: 2.14 -> 2.06 ms; the y passes are slower that way at 768^3)
+  static constexpr int kMinBlocksX = (E >= 24 ? 2 : 3) * 256 / kThreads;
   static constexpr size_t kSmem = sizeof(float2) * ((size_t)N + (size_t)kLineCols * LS);
   // the x pass holds the stage tables of both radix orders and the x axis's
   // Green's-function and k^2 tables (read from shared memory, not L1)
@@ -765,7 +769,7 @@ __global__ void __launch_bounds__(LineCfg<N>::kThreads, LineCfg<N>::kMinBlocks)
 // spectrum of the line does not go through shared memory between the two.
 // tw: the forward plan's stage tables, then the reversed plan's (N each).
 template <int N>
-__global__ void __launch_bounds__(LineCfg<N>::kThreads, LineCfg<N>::kMinBlocks)
+__global__ void __launch_bounds__(LineCfg<N>::kThreads, LineCfg<N>::kMinBlocksX)
     k_line_x_green(float2* __restrict__ Y, int Sz, const float2* __restrict__ tw, const float* __restrict__ gt,
                    const float* __restrict__ k2tab, float norm) {
   using L = LineCfg<N>;
