@@ -9,7 +9,7 @@ import re
 import pytest
 
 from tigerpm_b200 import _lib
-from tigerpm_b200.api import options_for, process_options
+from tigerpm_b200.api import make_options, options_for, process_options
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -55,6 +55,21 @@ def test_options_parse_flags():
         process_options(["--no_such_flag=1"])
     with pytest.raises(_lib.TPMError):
         process_options(["--assign=ngp"])
+
+
+def test_deposit_accumulator_option():
+    """deterministic_deposit selects the deposit accumulator: 0 FP32 atomics
+    (default), 1 exact int64, 2 26-bit fixed point; the header's constants
+    match."""
+    assert process_options(["--parts_dim=64", "--four_dim=64"]).deterministic_deposit == 0
+    for v in (0, 1, 2):
+        o = process_options(["--parts_dim=64", "--four_dim=64", f"--deterministic_deposit={v}"])
+        assert o.deterministic_deposit == v
+        assert make_options(16, 32, deterministic_deposit=v).deterministic_deposit == v
+    assert make_options(16, 32, deterministic_deposit=True).deterministic_deposit == 1
+    text = open(os.path.join(ROOT, "include", "tpm.h")).read()
+    for name, v in (("TPM_DEPOSIT_FP32", 0), ("TPM_DEPOSIT_EXACT64", 1), ("TPM_DEPOSIT_FIXED32", 2)):
+        assert re.search(rf"#define {name} {v}\b", text), name
 
 
 def test_error_strings(lib):
